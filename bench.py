@@ -1,0 +1,319 @@
+"""Benchmark: particle-steps/s of the fused push + trilinear gather.
+
+Workload (default): RF-gap protons -- 1e7 protons, 1 MeV +-1 %, 256^3 float32
+E+B map over a 20 cm cube (Ez = 5 MV/m gap profile, Bz = 0.2 T), E modulated
+by cos(2 pi 100 MHz t + phi_i), dt = 1e-11 s, 2e4 steps, snapshots every 500
+steps.  One bench "step" is one whole tracking job of that workload (all
+2e4 pushes of all particles, 41 snapshot writes), restarted from the same
+initial state, with inputs resident in HBM.  ``value`` is the mixed-precision
+form; the float64 plain form is timed the same way and reported beside it
+with the ratio and the mixed form's error against it (the float64 GPU path
+matches the reference to 1e-10).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun with N > 1 every rank runs an independent replica of the job
+(particles are independent: no data-path collective); value = total
+particle-steps of all ranks / max over ranks of the device time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=10_000_000)
+    ap.add_argument("--nsteps", type=int, default=20_000)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--sort-every", type=int, default=0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def measured_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline_sample(wl_fn, n_sample, steps, cores_hint):
+    """Time the CPU restatement of the reference algorithm on a bounded sample."""
+    from oracle import cpu_baseline
+    return cpu_baseline.run(wl_fn, n_sample, steps)
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    from oracle import cpu_baseline
+    res = cpu_baseline.run_reference_arm(args.n, args.nsteps, args.steps, args.warmup)
+    print(json.dumps(res), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from pypatools_b200 import workloads, PusherGPU, Field, RFModulation
+    from pypatools_b200.device_fields import DeviceFields
+    from pypatools_b200.pusher import DeviceTracker
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    wl = workloads.rf_gap_protons(n=args.n, nsteps=args.nsteps)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    efield = Field.from_arrays(g, wl.e_values)
+    bfield = Field.from_arrays(g, wl.b_values)
+    omega = 2 * np.pi * wl.rf_frequency
+    d_r0 = torch.from_numpy(wl.r0).to(dev)
+    d_v0 = torch.from_numpy(wl.v0).to(dev)
+    d_phase = torch.from_numpy(wl.rf_phase).to(dev)
+    chunk = wl.rec_every
+    n = wl.n
+
+    def run_form(precision):
+        df = DeviceFields(efield, bfield, precision, dev)
+        tr = DeviceTracker("boris", wl.species.q_over_m, df, n, wl.nsteps, wl.dt, wl.rec_every, precision,
+                           rf_omega=omega, rf_phase=d_phase, record=True, counters=True, device=dev)
+        stream = torch.cuda.current_stream()
+        launch_ev = []
+
+        def job(time_launches):
+            tr.step = 0
+            tr.order = None
+            tr.rf_phase.copy_(d_phase)
+            tr.load(d_r0, d_v0)
+            done = 0
+            while done < wl.nsteps:
+                if args.sort_every and done and done % args.sort_every == 0:
+                    tr.sort()
+                k = min(chunk, wl.nsteps - done)
+                if time_launches:
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    tr.advance(k)
+                    b.record(stream)
+                    launch_ev.append((a, b))
+                else:
+                    tr.advance(k)
+                done += k
+
+        for _ in range(args.warmup):
+            job(False)
+        torch.cuda.synchronize()
+        tr.counters.zero_()
+        launches0 = tr.launches
+        barrier()
+        torch.cuda.synchronize()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            job(True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = t0.elapsed_time(t1)
+        if world > 1:
+            tt = torch.tensor([ms], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        cnt = tr.counter_values()
+        launch_ms = [a.elapsed_time(b) for a, b in launch_ev]
+        out = {"ms_total": ms, "ms_per_job": ms / args.steps, "launch_ms": launch_ms,
+               "counters": cnt, "launches": tr.launches - launches0, "map_bytes": df.map_bytes,
+               "n_comp": df.n_components}
+        return tr, df, out
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    results = {}
+    r_fp64 = None
+    if not args.no_fp64:
+        tr64, df64, results["fp64"] = run_form("fp64")
+        r_fp64 = tr64.r_hist
+        v_fp64 = tr64.v_hist
+        del tr64, df64
+    trm, dfm, results["mixed"] = run_form("mixed")
+    clocks = sampler.stop()
+
+    # mixed-form error against the float64 form (which matches the oracle to 1e-10)
+    err = None
+    if r_fp64 is not None:
+        half = 0.5 * float(wl.grid[0][-1] - wl.grid[0][0])
+        num = torch.linalg.vector_norm(trm.r_hist - r_fp64, dim=2)
+        den = torch.clamp(torch.linalg.vector_norm(r_fp64, dim=2), min=half)
+        rel = (num / den).flatten()
+        vrel = (torch.linalg.vector_norm(trm.v_hist - v_fp64, dim=2) /
+                torch.linalg.vector_norm(v_fp64, dim=2)).flatten()
+        err = {"max_rel_pos": float(rel.max()), "p99_rel_pos": float(torch.quantile(rel[:: max(1, rel.numel() // 4_000_000)], 0.99)),
+               "max_rel_vel": float(vrel.max()), "against": "float64 GPU form (pinned to the oracle at 1e-10)"}
+        del r_fp64, v_fp64
+
+    total_ps = n * wl.nsteps * args.steps * world
+    m = results["mixed"]
+    value = total_ps / (m["ms_total"] / 1e3)
+
+    # roofline of the dominant kernel (mixed track kernel): algorithmic bytes
+    # = in-map gathers x 8 corners x stored components x 4 B + state in/out
+    # per launch + snapshot rows written.
+    peak, peak_kind = measured_peaks()
+    hits = m["counters"]["map_hits"]
+    n_launch = len(m["launch_ms"])
+    gather_b = hits * 8 * m["n_comp"] * 4
+    state_b = n_launch * n * 2 * 48
+    snap_b = args.steps * (wl.nsteps // wl.rec_every + 1) * n * 48
+    alg_bytes_per_launch = (gather_b + state_b + snap_b) / max(n_launch, 1)
+    avg_launch_s = float(np.mean(m["launch_ms"])) / 1e3
+    achieved = alg_bytes_per_launch / avg_launch_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs",
+                "kernel": "track_mixed_kernel<BORIS,RF>", "avg_launch_ms": avg_launch_s * 1e3,
+                "in_map_fraction": hits / max(1, m["counters"]["particle_steps"]),
+                "note": "gathers only for in-map particle-steps; the rest are register-only drift steps"}
+
+    # e2e through the public API with host buffers (H2D of r0/v0/phase, D2H of the histories)
+    e2e = None
+    if not args.no_e2e:
+        del trm, dfm
+        torch.cuda.empty_cache()
+        pusher = PusherGPU(wl.species, "boris", precision="mixed", steps_per_launch=chunk)
+        rf = RFModulation(wl.rf_frequency, wl.rf_phase)
+        for _ in range(1):
+            pusher.track_batch(wl.r0, wl.v0, efield, bfield, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            rh, vh, _ = pusher.track_batch(wl.r0, wl.v0, efield, bfield, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
+        dt_e2e = time.perf_counter() - t
+        n_rec = wl.nsteps // wl.rec_every + 1
+        # per step: r0 and v0 (n,3) float64 plus the n RF phases in; both
+        # (n_rec, n, 3) float64 histories out
+        e2e = {"value": n * wl.nsteps * args.e2e_steps * world / dt_e2e, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": int(2 * n * 24 + n * 8),
+               "d2h_bytes_per_step": int(2 * n_rec * n * 24),
+               "api": "PusherGPU.track_batch (numpy in, numpy histories out)", "steps": args.e2e_steps}
+        del rh, vh
+
+    cpu = None
+    if rank == 0:
+        from oracle import cpu_baseline
+        cpu = cpu_baseline.sample(n_sample=20_000, steps=20, in_map_fraction=roofline["in_map_fraction"])
+
+    if rank == 0:
+        f64 = results.get("fp64")
+        line = {
+            "metric": "particle-steps/s, mixed-precision fused Boris + trilinear E/B (RF gap, 1e7 protons, 256^3 map)",
+            "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": m["ms_per_job"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 time/phase, float-float velocity)",
+            "data": "synthetic (seeded pypatools_b200.workloads.rf_gap_protons)",
+            "config": {"workload": "rf_gap_protons", "particles_per_gpu": n, "steps_per_job": wl.nsteps,
+                       "dt": wl.dt, "map": "256^3 float32 E+B over a 20 cm cube", "rf_hz": wl.rf_frequency,
+                       "snapshot_every": wl.rec_every, "algorithm": "boris", "precision": "mixed",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (map 537 MB, state 480 MB, snapshots 19.7 GB)"},
+            "fp64": ({"value": total_ps / (f64["ms_total"] / 1e3), "ms_per_step": f64["ms_per_job"],
+                      "launches": f64["launches"]} if f64 else None),
+            "mixed_over_fp64": (f64["ms_total"] / m["ms_total"]) if f64 else None,
+            "error_vs_fp64": err,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": m["launches"],
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

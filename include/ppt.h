@@ -1,0 +1,204 @@
+/*
+ * ppt.h -- C ABI of libppt.so, the B200 (sm_100a) particle pusher with fused
+ * trilinear E/B field-map interpolation.
+ *
+ * Every entry point returns an int status (PPT_OK = 0, negative PPT_ERR_*),
+ * never throws, and leaves a thread-local message for ppt_last_error().
+ * Device work is ordered on the caller's stream (a cudaStream_t passed as
+ * void*; NULL = the legacy default stream).  All particle arrays, snapshot
+ * buffers and outputs are caller-owned DEVICE memory; the library never frees
+ * them.  Field maps are library-owned device copies behind an opaque handle.
+ *
+ * Reference interfaces each group replaces (DanielWinklehner/PyPATools,
+ * paths inside that project):
+ *   ppt_fieldmap_*  Field.from_arrays / get_interpolator / NumbaInterpolator
+ *                   construction (src/PyPATools/field.py:345-387,
+ *                   src/PyPATools/field_src/interpolators.py:299-347, :533-610)
+ *   ppt_field_eval  Field.__call__ -> _get_field_3d -> NumbaInterpolator.__call__
+ *                   -> _interp3d_batch (field.py:213-244, :491-504,
+ *                   interpolators.py:349-402, :259-267, :88-135)
+ *   ppt_track       Pusher.track_batch's step loop with push_batch and the
+ *                   per-algorithm batch kernels (src/PyPATools/pusher.py:894-1012,
+ *                   :699-801, :369-404, :803-892)
+ *   ppt_state_*     the (M,3) float64 r/v arrays track_batch takes and returns
+ *                   (pusher.py:934-962, :1012)
+ *   ppt_moments     ParticleDistribution statistics (src/PyPATools/particles.py:
+ *                   693-719, :761-788, :507-525, :393-457)
+ *   ppt_cell_sort   no reference counterpart: particle reordering for gather
+ *                   locality (the reference has no particle ordering step)
+ */
+#ifndef PPT_H
+#define PPT_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PPT_ABI_VERSION 1
+
+/* status codes */
+#define PPT_OK               0
+#define PPT_ERR_ARG         -1   /* bad argument (null pointer, size, enum) */
+#define PPT_ERR_OOM         -2   /* device allocation failed */
+#define PPT_ERR_CUDA        -3   /* a CUDA runtime call failed */
+#define PPT_ERR_UNSUPPORTED -4   /* valid request this build does not handle */
+#define PPT_ERR_TIMEOUT     -5   /* a bounded device wait expired */
+#define PPT_ERR_DEVICE      -6   /* the device status word reported a fault */
+
+/* Algorithms: the reference's Pusher.ALGORITHMS order (pusher.py:465-466),
+ * then two additions that conserve |u| in a pure magnetic field. */
+#define PPT_ALG_LEAPFROG     0
+#define PPT_ALG_BORIS        1   /* non-relativistic Boris, pusher.py:124-165 */
+#define PPT_ALG_RK4          2
+#define PPT_ALG_YOSHIDA      3
+#define PPT_ALG_VAY_REL      4   /* the reference's 'vay_rel' as written, pusher.py:216-279 */
+#define PPT_ALG_RK4_REL      5
+#define PPT_ALG_YOSHIDA_REL  6
+#define PPT_ALG_BORIS_REL    7   /* relativistic Boris in u = gamma v (addition) */
+#define PPT_ALG_VAY          8   /* Vay (2008) as published (addition) */
+#define PPT_ALG_COUNT        9
+
+/* Precision forms */
+#define PPT_PREC_F64    0   /* the reference method in float64 (the drop-in) */
+#define PPT_PREC_MIXED  1   /* int cell + float32 offset, float32 gathers and
+                               rotation, float-float velocity accumulation */
+
+/* Element types */
+#define PPT_DTYPE_F64 0
+#define PPT_DTYPE_F32 1
+
+/* Track flags */
+#define PPT_TRACK_INIT   1   /* this call starts the track: Boris-family
+                                half step back and record 0 */
+#define PPT_TRACK_FINAL  2   /* this call ends the track: Boris-family final
+                                half step, v of the last record overwritten */
+
+/* Device status bits (OR-ed into *status) */
+#define PPT_STATUS_NONFINITE  1  /* a particle's state became NaN/Inf */
+#define PPT_STATUS_BOUNDS     2  /* a debug-build bounds check failed */
+
+#define PPT_MAX_MAPS 4
+
+typedef struct ppt_fieldmap ppt_fieldmap;   /* opaque */
+
+/* Node grid of one map: n[d] >= 2 sorted node coordinates per axis, given
+ * as HOST arrays (copied).  Node values are indexed [i][j][k] with k
+ * fastest, the 'ij' meshgrid order NumbaInterpolator uses. */
+typedef struct {
+    int64_t n[3];
+    const double* axis[3];
+} ppt_grid_desc;
+
+/* Create a zero-valued map on the current device.  has_e / has_b say which
+ * fields it stores; store_dtype is PPT_DTYPE_F64 (plain form) or
+ * PPT_DTYPE_F32 (mixed form, needs uniform axes). */
+int ppt_fieldmap_create(const ppt_grid_desc* grid, int has_e, int has_b, int store_dtype,
+                        ppt_fieldmap** out);
+
+/* map += scale[c] * comp[c] for c in (Ex,Ey,Ez,Bx,By,Bz).  comp[c] is a
+ * DEVICE pointer to an n[0]*n[1]*n[2] C-contiguous array of src_dtype, or
+ * NULL (adds nothing).  Used once per term of a composite / scaled field. */
+int ppt_fieldmap_add(ppt_fieldmap* map, const void* const comp[6], const double scale[6],
+                     int src_dtype, void* stream);
+
+int ppt_fieldmap_destroy(ppt_fieldmap* map);
+
+/* bytes of device memory held, and flags: bit0 has_e, bit1 has_b,
+ * bit2 all axes uniform, bit3 float32 storage */
+int ppt_fieldmap_info(const ppt_fieldmap* map, int64_t* bytes, int* flags);
+
+/* The fields a pusher sees: E = e_const + sum over maps of the map's E,
+ * B likewise; maps outside their grid contribute 0 (fill_value = 0,
+ * field.py:337-338). */
+typedef struct {
+    const ppt_fieldmap* maps[PPT_MAX_MAPS];
+    int32_t n_maps;
+    double e_const[3];
+    double b_const[3];
+} ppt_fields;
+
+/* E and B at n points.  pts: device (n,3) float64; e_out, b_out: device
+ * (n,3) float64 (either may be NULL). */
+int ppt_field_eval(const ppt_fields* fields, int64_t n, const double* pts,
+                   double* e_out, double* b_out, void* stream);
+
+/* Particle state on the device, structure of arrays:
+ *   PPT_PREC_F64:   f64[6*n]  = x | y | z | w_x | w_y | w_z
+ *   PPT_PREC_MIXED: i32[3*n]  = cell i | j | k  (on map 0's grid)
+ *                   f32[9*n]  = offset x|y|z | w_hi x|y|z | w_lo x|y|z
+ * w is the velocity v [m/s], or u = gamma v for BORIS_REL / VAY. */
+typedef struct {
+    int32_t precision;
+    int32_t algorithm;
+    int64_t n;
+    double* f64;
+    int32_t* i32;
+    float* f32;
+} ppt_state;
+
+/* Fill the state from (n,3) float64 r [m] and v [m/s] (device, row-major).
+ * The mixed form locates cells on fields->maps[0]'s grid. */
+int ppt_state_load(ppt_state* st, const ppt_fields* fields, const double* r, const double* v,
+                   void* stream);
+
+/* Write the state back as (n,3) float64 r and v (v = u/gamma for u-state
+ * algorithms).  order (device int64[n], or NULL) maps slot -> row. */
+int ppt_state_store(const ppt_state* st, const ppt_fields* fields, const int64_t* order,
+                    double* r, double* v, void* stream);
+
+typedef struct {
+    int64_t step0;        /* global index of this call's first step */
+    int64_t nsteps;       /* steps in this call */
+    int64_t nsteps_total; /* steps of the whole track (record count, final half step) */
+    int64_t rec_every;    /* record every N steps (>= 1) */
+    int32_t flags;        /* PPT_TRACK_INIT | PPT_TRACK_FINAL */
+    int32_t reserved;
+    double dt;
+    double q_over_m;
+    double t0;            /* field time of step 0 */
+    double rf_omega;      /* E multiplied by cos(rf_omega t + rf_phase[i]) ... */
+    const double* rf_phase; /* ... when non-NULL: device float64 [n], in state (slot) order */
+    double* r_hist;       /* device (nsteps_total/rec_every + 1, n, 3) or NULL */
+    double* v_hist;
+    const int64_t* order; /* slot -> row (after ppt_cell_sort), NULL = identity */
+    int32_t* status;      /* device int32, OR-ed with PPT_STATUS_* bits, or NULL */
+    unsigned long long* counters; /* device u64[2]: +in-map gathers, +particle steps; or NULL */
+} ppt_track_args;
+
+/* Advance every particle nsteps steps in ONE kernel launch, state kept in
+ * registers, fields gathered on the fly, snapshots written into r_hist /
+ * v_hist at the reference's record indices. */
+int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_track_args* args, void* stream);
+
+/* Reorder particles by cell (locality of the corner gathers).  Permutes the
+ * state, rf_phase and order arrays in place.  Needs n_cells_hint >= 1.
+ * scratch: device buffer of ppt_cell_sort_scratch_bytes(n) bytes. */
+int64_t ppt_cell_sort_scratch_bytes(int64_t n);
+int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* order, double* rf_phase,
+                  void* scratch, void* stream);
+
+/* Bunch moments of n particles from (n,3) float64 positions and velocities
+ * (device), in float64:
+ *   out[0..2]   centroid            out[3..5]   x_std
+ *   out[6..8]   xp_std              out[9..11]  xp_mean
+ *   out[12..15] xxp yyp xyp yxp     out[16]     mean |p| (beta gamma)
+ *   out[17..19] mean p              out[20]     mean Ekin [MeV]
+ *   out[21]     std Ekin [MeV]
+ * Velocities go through the reference's per-component v -> p -> v
+ * conversion first.  scratch: device buffer of ppt_moments_scratch_bytes(n). */
+#define PPT_MOMENTS_LEN 22
+int64_t ppt_moments_scratch_bytes(int64_t n);
+int ppt_moments(int64_t n, const double* r, const double* v, double mass_mev,
+                double* out, void* scratch, void* stream);
+
+const char* ppt_last_error(void);
+int ppt_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PPT_H */

@@ -1,0 +1,113 @@
+"""ctypes binding of libppt.so (the C ABI declared in include/ppt.h).
+
+The library is the only compute path: if it is missing or fails to load,
+importing the GPU entry points raises instead of falling back to the CPU.
+"""
+import ctypes
+import os
+from ctypes import c_double, c_int, c_int32, c_int64, c_void_p, POINTER
+from pathlib import Path
+
+LIB_PATH = Path(os.environ.get("PPT_LIBRARY", Path(__file__).resolve().parent / "lib" / "libppt.so"))
+
+PPT_OK = 0
+ERRORS = {-1: "PPT_ERR_ARG", -2: "PPT_ERR_OOM", -3: "PPT_ERR_CUDA", -4: "PPT_ERR_UNSUPPORTED",
+          -5: "PPT_ERR_TIMEOUT", -6: "PPT_ERR_DEVICE"}
+
+ALG_IDS = {"leapfrog": 0, "boris": 1, "rk4": 2, "yoshida": 3, "vay_rel": 4, "rk4_rel": 5,
+           "yoshida_rel": 6, "boris_rel": 7, "vay": 8}
+PREC_F64, PREC_MIXED = 0, 1
+DTYPE_F64, DTYPE_F32 = 0, 1
+TRACK_INIT, TRACK_FINAL = 1, 2
+STATUS_NONFINITE, STATUS_BOUNDS = 1, 2
+MAX_MAPS = 4
+MOMENTS_LEN = 22
+
+
+class PptError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class PptUnsupported(PptError, NotImplementedError):
+    pass
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("n", c_int64 * 3), ("axis", c_void_p * 3)]
+
+
+class Fields(ctypes.Structure):
+    _fields_ = [("maps", c_void_p * MAX_MAPS), ("n_maps", c_int32),
+                ("e_const", c_double * 3), ("b_const", c_double * 3)]
+
+
+class State(ctypes.Structure):
+    _fields_ = [("precision", c_int32), ("algorithm", c_int32), ("n", c_int64),
+                ("f64", c_void_p), ("i32", c_void_p), ("f32", c_void_p)]
+
+
+class TrackArgs(ctypes.Structure):
+    _fields_ = [("step0", c_int64), ("nsteps", c_int64), ("nsteps_total", c_int64),
+                ("rec_every", c_int64), ("flags", c_int32), ("reserved", c_int32),
+                ("dt", c_double), ("q_over_m", c_double), ("t0", c_double),
+                ("rf_omega", c_double), ("rf_phase", c_void_p), ("r_hist", c_void_p),
+                ("v_hist", c_void_p), ("order", c_void_p), ("status", c_void_p),
+                ("counters", c_void_p)]
+
+
+# name -> (restype, argtypes); every symbol include/ppt.h declares
+SIGNATURES = {
+    "ppt_fieldmap_create": (c_int, [POINTER(GridDesc), c_int, c_int, c_int, POINTER(c_void_p)]),
+    "ppt_fieldmap_add": (c_int, [c_void_p, POINTER(c_void_p * 6), POINTER(c_double * 6), c_int, c_void_p]),
+    "ppt_fieldmap_destroy": (c_int, [c_void_p]),
+    "ppt_fieldmap_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int)]),
+    "ppt_field_eval": (c_int, [POINTER(Fields), c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "ppt_state_load": (c_int, [POINTER(State), POINTER(Fields), c_void_p, c_void_p, c_void_p]),
+    "ppt_state_store": (c_int, [POINTER(State), POINTER(Fields), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "ppt_track": (c_int, [POINTER(State), POINTER(Fields), POINTER(TrackArgs), c_void_p]),
+    "ppt_cell_sort_scratch_bytes": (c_int64, [c_int64]),
+    "ppt_cell_sort": (c_int, [POINTER(State), POINTER(Fields), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "ppt_moments_scratch_bytes": (c_int64, [c_int64]),
+    "ppt_moments": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
+    "ppt_last_error": (ctypes.c_char_p, []),
+    "ppt_abi_version": (c_int, []),
+}
+
+_lib = None
+
+
+def load():
+    """Load libppt.so once; raise loudly when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m pypatools_b200.build` "
+                          "(there is no CPU fallback for the pusher path)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.ppt_abi_version() != 1:
+        raise ImportError("libppt.so ABI version mismatch; rebuild it")
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != PPT_OK:
+        msg = load().ppt_last_error().decode("utf-8", "replace")
+        if rc == -4:
+            raise PptUnsupported(rc, msg)
+        raise PptError(rc, msg)
+    return rc
+
+
+def stream_handle(stream=None):
+    """cudaStream_t of a torch stream (current stream by default) as int."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

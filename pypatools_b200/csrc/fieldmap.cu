@@ -1,0 +1,276 @@
+// Field maps: upload/accumulate of node values into the interleaved device
+// layout, and standalone E/B evaluation at arbitrary points.
+//
+// Reference behaviour restated here:
+//   Field.from_arrays builds one NumbaInterpolator per component on the
+//   shared grid, values copied to contiguous float64
+//   (src/PyPATools/field.py:345-387, field_src/interpolators.py:299-347);
+//   Field.__call__ -> _get_field_3d evaluates the three components and
+//   multiplies by the field's scaling (field.py:213-244, :491-504).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ppt_internal.cuh"
+
+namespace ppt {
+
+int grid_for(int64_t n, int block) {
+    int64_t g = (n + block - 1) / block;
+    return (int)(g < 1 ? 1 : g);
+}
+
+// Small particle counts (the 4096-particle case) would put all blocks on a
+// handful of SMs; narrower blocks spread them over the 148 SMs.
+int pick_block(int64_t n) {
+    if (n <= 148LL * 32) return 32;
+    if (n <= 148LL * 64 * 2) return 64;
+    return 128;
+}
+
+// ---------------------------------------------------------------------------
+// accumulate kernel: map[node][slot] += scale * src[node]
+// ---------------------------------------------------------------------------
+template <typename Dst, typename Src>
+__global__ void map_add_kernel(Dst* __restrict__ dst, int stride, int slot,
+                               const Src* __restrict__ src, double scale, int64_t nodes) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    for (; i < nodes; i += step) {
+        Dst* p = dst + i * stride + slot;
+        *p = (Dst)((double)*p + scale * (double)src[i]);
+    }
+}
+
+int build_fields(const ppt_fields* f, FieldsDev* out) {
+    if (!f) return fail(PPT_ERR_ARG, "fields is NULL");
+    if (f->n_maps < 0 || f->n_maps > PPT_MAX_MAPS)
+        return fail(PPT_ERR_ARG, "n_maps must be in [0, PPT_MAX_MAPS]");
+    std::memset(out, 0, sizeof(*out));
+    out->n_maps = f->n_maps;
+    for (int i = 0; i < f->n_maps; ++i) {
+        if (!f->maps[i]) return fail(PPT_ERR_ARG, "fields->maps[i] is NULL");
+        out->maps[i] = f->maps[i]->dev;
+        out->e_maps += out->maps[i].has_e;
+        out->b_maps += out->maps[i].has_b;
+    }
+    for (int c = 0; c < 3; ++c) {
+        out->e_const[c] = f->e_const[c];
+        out->b_const[c] = f->b_const[c];
+        out->e_const_nz |= (f->e_const[c] != 0.0);
+        out->b_const_nz |= (f->b_const[c] != 0.0);
+    }
+    return PPT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// point evaluation kernel (the 'cuda' interpolator backend)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float tri_f(float c000, float c100, float c010, float c110, float c001,
+                                       float c101, float c011, float c111, float tx, float ty, float tz);
+
+__global__ void field_eval_kernel(const __grid_constant__ FieldsDev F, int64_t n,
+                                  const double* __restrict__ pts, double* __restrict__ e_out,
+                                  double* __restrict__ b_out) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    V3 r = v3(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]);
+    V3 E = v3(F.e_const[0], F.e_const[1], F.e_const[2]);
+    V3 B = v3(F.b_const[0], F.b_const[1], F.b_const[2]);
+    for (int mi = 0; mi < F.n_maps; ++mi) {
+        const MapDev& m = F.maps[mi];
+        Cell c;
+        if (!locate(m, r, c)) continue;
+        if (m.dtype == PPT_DTYPE_F64) {
+            if (m.has_e) E = E + gather_f64(m, c, 0);
+            if (m.has_b) B = B + gather_f64(m, c, m.b_off);
+        } else {
+            const float* base = static_cast<const float*>(m.data);
+            float tx = (float)c.tx, ty = (float)c.ty, tz = (float)c.tz;
+            for (int h = 0; h < 2; ++h) {
+                if (h == 0 && !m.has_e) continue;
+                if (h == 1 && !m.has_b) continue;
+                int off = h == 0 ? 0 : m.b_off;
+                float4 q[8];
+                for (int k = 0; k < 8; ++k) {
+                    int di = (k >> 2) & 1, dj = (k >> 1) & 1, dk = k & 1;
+                    int64_t node = c.base + di * m.sx + dj * m.sy + dk;
+                    q[k] = __ldg(reinterpret_cast<const float4*>(base + node * m.stride + off));
+                }
+                V3 o = v3(tri_f(q[0].x, q[4].x, q[2].x, q[6].x, q[1].x, q[5].x, q[3].x, q[7].x, tx, ty, tz),
+                          tri_f(q[0].y, q[4].y, q[2].y, q[6].y, q[1].y, q[5].y, q[3].y, q[7].y, tx, ty, tz),
+                          tri_f(q[0].z, q[4].z, q[2].z, q[6].z, q[1].z, q[5].z, q[3].z, q[7].z, tx, ty, tz));
+                if (h == 0) E = E + o; else B = B + o;
+            }
+        }
+    }
+    if (e_out) { e_out[3 * p] = E.x; e_out[3 * p + 1] = E.y; e_out[3 * p + 2] = E.z; }
+    if (b_out) { b_out[3 * p] = B.x; b_out[3 * p + 1] = B.y; b_out[3 * p + 2] = B.z; }
+}
+
+__device__ __forceinline__ float tri_f(float c000, float c100, float c010, float c110, float c001,
+                                       float c101, float c011, float c111, float tx, float ty, float tz) {
+    float c00 = fmaf(c100 - c000, tx, c000);
+    float c01 = fmaf(c101 - c001, tx, c001);
+    float c10 = fmaf(c110 - c010, tx, c010);
+    float c11 = fmaf(c111 - c011, tx, c011);
+    float c0 = fmaf(c10 - c00, ty, c00);
+    float c1 = fmaf(c11 - c01, ty, c01);
+    return fmaf(c1 - c0, tz, c0);
+}
+
+}  // namespace ppt
+
+using namespace ppt;
+
+extern "C" int ppt_fieldmap_create(const ppt_grid_desc* grid, int has_e, int has_b, int store_dtype,
+                                   ppt_fieldmap** out) {
+    if (!grid || !out) return fail(PPT_ERR_ARG, "grid and out must not be NULL");
+    *out = nullptr;
+    if (!has_e && !has_b) return fail(PPT_ERR_ARG, "a map must store E, B or both");
+    if (store_dtype != PPT_DTYPE_F64 && store_dtype != PPT_DTYPE_F32)
+        return fail(PPT_ERR_ARG, "store_dtype must be PPT_DTYPE_F64 or PPT_DTYPE_F32");
+    ppt_fieldmap m;
+    std::memset(&m, 0, sizeof(m));
+    int64_t total_nodes = 1;
+    std::vector<double> axes;
+    for (int d = 0; d < 3; ++d) {
+        int64_t n = grid->n[d];
+        if (n < 2) return fail(PPT_ERR_ARG, "every axis needs at least 2 nodes");
+        if (n > (1LL << 30)) return fail(PPT_ERR_ARG, "axis too long");
+        if (!grid->axis[d]) return fail(PPT_ERR_ARG, "grid axis pointer is NULL");
+        const double* g = grid->axis[d];
+        for (int64_t i = 1; i < n; ++i)
+            if (!(g[i] > g[i - 1])) return fail(PPT_ERR_ARG, "grid axes must be strictly increasing");
+        AxisDev& a = m.dev.ax[d];
+        a.n = (int)n;
+        a.lo = g[0];
+        a.hi = g[n - 1];
+        a.d = (a.hi - a.lo) / (double)(n - 1);
+        a.inv_d = (double)(n - 1) / (a.hi - a.lo);
+        // Uniform when every node sits within 1e-12 cell widths of lo + i d:
+        // the weights then differ from the bisection ones by rounding only.
+        double worst = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            double dev = std::fabs(g[i] - (a.lo + (double)i * a.d));
+            worst = dev > worst ? dev : worst;
+        }
+        a.uniform = worst <= 1e-12 * a.d;
+        m.n[d] = n;
+        total_nodes *= n;
+        axes.insert(axes.end(), g, g + n);
+    }
+    m.dev.all_uniform = m.dev.ax[0].uniform && m.dev.ax[1].uniform && m.dev.ax[2].uniform;
+    if (store_dtype == PPT_DTYPE_F32 && !m.dev.all_uniform)
+        return fail(PPT_ERR_UNSUPPORTED, "float32 (mixed-precision) maps need uniform grid axes");
+    m.dev.has_e = has_e ? 1 : 0;
+    m.dev.has_b = has_b ? 1 : 0;
+    m.dev.stride = (has_e && has_b) ? 8 : 4;
+    m.dev.b_off = has_e ? 4 : 0;
+    m.dev.dtype = store_dtype;
+    m.dev.sy = m.n[2];
+    m.dev.sx = m.n[1] * m.n[2];
+    size_t elem = store_dtype == PPT_DTYPE_F64 ? 8 : 4;
+    m.bytes = (size_t)total_nodes * m.dev.stride * elem;
+    PPT_CUDA_TRY(cudaGetDevice(&m.device));
+    cudaError_t e = cudaMalloc(&m.data, m.bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(PPT_ERR_OOM, "cudaMalloc of the field map failed");
+    }
+    e = cudaMalloc(&m.axis_buf, axes.size() * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaFree(m.data);
+        cudaGetLastError();
+        return fail(PPT_ERR_OOM, "cudaMalloc of the grid axes failed");
+    }
+    e = cudaMemcpy(m.axis_buf, axes.data(), axes.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(m.data, 0, m.bytes);
+    if (e != cudaSuccess) {
+        cudaFree(m.data);
+        cudaFree(m.axis_buf);
+        return cuda_fail(e, "field map initialisation");
+    }
+    m.dev.data = m.data;
+    m.dev.ax[0].nodes = m.axis_buf;
+    m.dev.ax[1].nodes = m.axis_buf + m.n[0];
+    m.dev.ax[2].nodes = m.axis_buf + m.n[0] + m.n[1];
+    *out = new ppt_fieldmap(m);
+    return PPT_OK;
+}
+
+extern "C" int ppt_fieldmap_add(ppt_fieldmap* map, const void* const comp[6], const double scale[6],
+                                int src_dtype, void* stream) {
+    if (!map || !comp || !scale) return fail(PPT_ERR_ARG, "map, comp and scale must not be NULL");
+    if (src_dtype != PPT_DTYPE_F64 && src_dtype != PPT_DTYPE_F32)
+        return fail(PPT_ERR_ARG, "src_dtype must be PPT_DTYPE_F64 or PPT_DTYPE_F32");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t nodes = map->n[0] * map->n[1] * map->n[2];
+    const int block = 256;
+    int64_t g = (nodes + block - 1) / block;
+    const int grid = (int)(g > 148 * 32 ? 148 * 32 : g);
+    for (int c = 0; c < 6; ++c) {
+        if (!comp[c]) continue;
+        const bool is_e = c < 3;
+        if (is_e && !map->dev.has_e) return fail(PPT_ERR_ARG, "map does not store E");
+        if (!is_e && !map->dev.has_b) return fail(PPT_ERR_ARG, "map does not store B");
+        const int slot = (is_e ? 0 : map->dev.b_off) + (c % 3);
+        if (map->dev.dtype == PPT_DTYPE_F64) {
+            double* dst = static_cast<double*>(map->data);
+            if (src_dtype == PPT_DTYPE_F64)
+                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
+                                                      static_cast<const double*>(comp[c]), scale[c], nodes);
+            else
+                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
+                                                      static_cast<const float*>(comp[c]), scale[c], nodes);
+        } else {
+            float* dst = static_cast<float*>(map->data);
+            if (src_dtype == PPT_DTYPE_F64)
+                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
+                                                      static_cast<const double*>(comp[c]), scale[c], nodes);
+            else
+                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
+                                                      static_cast<const float*>(comp[c]), scale[c], nodes);
+        }
+        PPT_CUDA_TRY(cudaGetLastError());
+    }
+    return PPT_OK;
+}
+
+extern "C" int ppt_fieldmap_destroy(ppt_fieldmap* map) {
+    if (!map) return PPT_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(map->device);
+    cudaError_t e1 = cudaFree(map->data);
+    cudaError_t e2 = cudaFree(map->axis_buf);
+    cudaSetDevice(prev);
+    delete map;
+    if (e1 != cudaSuccess) return cuda_fail(e1, "cudaFree(field map)");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaFree(grid axes)");
+    return PPT_OK;
+}
+
+extern "C" int ppt_fieldmap_info(const ppt_fieldmap* map, int64_t* bytes, int* flags) {
+    if (!map) return fail(PPT_ERR_ARG, "map is NULL");
+    if (bytes) *bytes = (int64_t)map->bytes;
+    if (flags)
+        *flags = map->dev.has_e | (map->dev.has_b << 1) | (map->dev.all_uniform << 2) |
+                 ((map->dev.dtype == PPT_DTYPE_F32) << 3);
+    return PPT_OK;
+}
+
+extern "C" int ppt_field_eval(const ppt_fields* fields, int64_t n, const double* pts, double* e_out,
+                              double* b_out, void* stream) {
+    if (n < 0) return fail(PPT_ERR_ARG, "n must be >= 0");
+    if (n == 0) return PPT_OK;
+    if (!pts) return fail(PPT_ERR_ARG, "pts is NULL");
+    FieldsDev F;
+    int rc = build_fields(fields, &F);
+    if (rc) return rc;
+    const int block = 128;
+    field_eval_kernel<<<grid_for(n, block), block, 0, static_cast<cudaStream_t>(stream)>>>(F, n, pts, e_out,
+                                                                                           b_out);
+    PPT_CUDA_TRY(cudaGetLastError());
+    return PPT_OK;
+}

@@ -1,0 +1,321 @@
+// Plain form: the reference's pushers in float64, fused with the trilinear
+// gathers, many steps per launch.
+//
+// One thread owns one particle for the whole launch.  Its position and
+// velocity live in registers across all steps of the call; per step it
+// locates its cell, gathers the 8 corner records (one 256-bit load per field
+// per corner), interpolates E and B, applies the algorithm's update and
+// writes a snapshot row only on record steps.  The reference instead makes 6
+// (Boris/Vay) or 24 (RK4) separate interpolation passes per step over
+// particle arrays in DRAM, each with its own binary search
+// (src/PyPATools/pusher.py:966-980, :699-801, field.py:491-504).
+//
+// Arithmetic follows the reference's kernels term by term so the results
+// agree to rounding: Boris pusher.py:124-165, Vay 'vay_rel' :216-279,
+// relativistic gamma :74-96, RK4 :803-892 with derivatives :168-172 and
+// :282-298, leapfrog :730-739, Yoshida :184-209 / :332-362 (fields frozen at
+// the step start), |v| clamps :275-277 / :886-890.  boris_rel and vay are
+// additions (u = gamma v state, see the oracle for their equations).
+#include <cmath>
+
+#include "track_params.cuh"
+
+namespace ppt {
+
+
+__host__ __device__ constexpr bool alg_staggered(int a) {
+    return a == PPT_ALG_BORIS || a == PPT_ALG_BORIS_REL || a == PPT_ALG_VAY;
+}
+__host__ __device__ constexpr bool alg_u_state(int a) { return a == PPT_ALG_BORIS_REL || a == PPT_ALG_VAY; }
+
+// Yoshida (1990) 4th-order coefficients, the float64 values of the
+// reference's expressions (pusher.py:176-181), written to round-trip exactly.
+constexpr double kYoC1 = 1.3512071919596578;     // 1 / (2 - 2^(1/3))
+constexpr double kYoC2 = -1.7024143839193153;    // -2^(1/3) / (2 - 2^(1/3))
+constexpr double kYoD1 = 2.7024143839193155;     // 2 C1
+constexpr double kYoD2 = -3.0536215758789735;    // -(2^(1/3) + 1) / (2 - 2^(1/3))
+
+// ---------------------------------------------------------------------------
+// per-algorithm updates (float64)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double rel_gamma(V3 v) {
+    double bsq = dot(v, v) / (kClight * kClight);
+    if (bsq >= 0.9999) bsq = 0.9999;
+    return 1.0 / sqrt(1.0 - bsq);
+}
+
+__device__ __forceinline__ V3 clamp_speed(V3 v) {
+    double vm = sqrt(dot(v, v));
+    if (vm >= 0.9999 * kClight) v = v * (0.9999 * kClight / vm);
+    return v;
+}
+
+__device__ __forceinline__ V3 boris_v(V3 v, V3 E, V3 B, double dt, double qm) {
+    const double h = 0.5 * qm;
+    V3 kick = v3(h * E.x * dt, h * E.y * dt, h * E.z * dt);
+    V3 vm = v + kick;
+    V3 t = v3(h * B.x * dt, h * B.y * dt, h * B.z * dt);
+    double f = 2.0 / (1.0 + (t.x * t.x + t.y * t.y + t.z * t.z));
+    V3 s = t * f;
+    V3 vp = vm + cross(vm, t);
+    V3 vplus = vm + cross(vp, s);
+    return vplus + kick;
+}
+
+__device__ __forceinline__ V3 vay_rel_v(V3 v, V3 E, V3 B, double dt, double qm) {
+    double g = rel_gamma(v);
+    V3 u = g * v;
+    V3 tau = v3(0.5 * qm * B.x * dt, 0.5 * qm * B.y * dt, 0.5 * qm * B.z * dt);
+    V3 up = v3(u.x + qm * E.x * dt, u.y + qm * E.y * dt, u.z + qm * E.z * dt);
+    double upm = sqrt(dot(up, up));
+    double taum = sqrt(dot(tau, tau));
+    double udt = dot(up, tau);
+    double gis = 1.0 - (upm / kClight) * (upm / kClight);
+    if (gis < 1e-10) gis = 1e-10;
+    double sigma = gis - taum * taum;
+    double q = udt / kClight;
+    double gn = sqrt(0.5 * (sigma + sqrt(sigma * sigma + 4.0 * (taum * taum + q * q))));
+    double ig = 1.0 / gn;
+    V3 t = tau * ig;
+    double f = 2.0 / (1.0 + taum * taum * (ig * ig));
+    V3 s = t * f;
+    V3 us = up + cross(up, t);
+    V3 un = up + cross(us, s);
+    return clamp_speed(un * ig);
+}
+
+__device__ __forceinline__ V3 lorentz(V3 v, V3 E, V3 B, double qm) { return qm * (E + cross(v, B)); }
+
+__device__ __forceinline__ V3 rk4_rel_deriv(V3 v, V3 E, V3 B, double qm) {
+    double g = rel_gamma(v);
+    V3 F = qm * (E + cross(v, B));
+    double vdf = dot(v, F);
+    V3 corr = (vdf / (g * kClight * kClight)) * v;
+    return F / g - corr;
+}
+
+__device__ __forceinline__ double gamma_u(V3 u) { return sqrt(1.0 + dot(u, u) / (kClight * kClight)); }
+
+__device__ __forceinline__ V3 boris_rel_u(V3 u, V3 E, V3 B, double dt, double qm) {
+    const double h = 0.5 * qm * dt;
+    V3 um = u + h * E;
+    double g = gamma_u(um);
+    V3 t = (h / g) * B;
+    double f = 2.0 / (1.0 + dot(t, t));
+    V3 s = t * f;
+    V3 up = um + cross(um, t);
+    V3 uplus = um + cross(up, s);
+    return uplus + h * E;
+}
+
+__device__ __forceinline__ V3 vay_u(V3 u, V3 E, V3 B, double dt, double qm) {
+    double g_old = gamma_u(u);
+    V3 v_old = u / g_old;
+    V3 up = u + (qm * dt) * (E + 0.5 * cross(v_old, B));
+    V3 tau = (0.5 * qm * dt) * B;
+    double tau_sq = dot(tau, tau);
+    double ustar = dot(up, tau) / kClight;
+    double sigma = 1.0 + dot(up, up) / (kClight * kClight) - tau_sq;
+    double gn = sqrt(0.5 * (sigma + sqrt(sigma * sigma + 4.0 * (tau_sq + ustar * ustar))));
+    V3 t = tau / gn;
+    double s = 1.0 / (1.0 + dot(t, t));
+    return s * (up + dot(up, t) * t + cross(up, t));
+}
+
+template <int ALG>
+__device__ __forceinline__ V3 w_to_v(V3 w) {
+    if constexpr (alg_u_state(ALG)) return w / gamma_u(w);
+    else return w;
+}
+
+template <int ALG>
+__device__ __forceinline__ V3 half_kick(V3 w, V3 E, V3 B, double dt, double qm) {
+    if constexpr (ALG == PPT_ALG_BORIS) return boris_v(w, E, B, dt, qm);
+    else if constexpr (ALG == PPT_ALG_BORIS_REL) return boris_rel_u(w, E, B, dt, qm);
+    else return vay_u(w, E, B, dt, qm);
+}
+
+struct Ctx {
+    const FieldsDev* F;
+    double dt, qm, omega, phase;
+    unsigned hits;
+};
+
+template <bool RF>
+__device__ __forceinline__ void fields_at(Ctx& c, V3 r, double t, V3& E, V3& B) {
+    c.hits += eval_fields_f64(*c.F, r, E, B);
+    if (RF) {
+        if (E.x != 0.0 || E.y != 0.0 || E.z != 0.0) E = E * cos(c.omega * t + c.phase);
+    }
+}
+
+template <int ALG, bool RF>
+__device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, double t) {
+    const double dt = c.dt, qm = c.qm;
+    if constexpr (ALG == PPT_ALG_RK4 || ALG == PPT_ALG_RK4_REL) {
+        constexpr bool REL = ALG == PPT_ALG_RK4_REL;
+        V3 E, B;
+        const double h = 0.5 * dt;
+        fields_at<RF>(c, r, t, E, B);
+        V3 k1v = REL ? rk4_rel_deriv(w, E, B, qm) : lorentz(w, E, B, qm);
+        V3 k1r = w;
+        V3 r2 = r + h * k1r, v2 = w + h * k1v;
+        fields_at<RF>(c, r2, t + h, E, B);
+        V3 k2v = REL ? rk4_rel_deriv(v2, E, B, qm) : lorentz(v2, E, B, qm);
+        V3 r3 = r + h * v2, v3_ = w + h * k2v;
+        fields_at<RF>(c, r3, t + h, E, B);
+        V3 k3v = REL ? rk4_rel_deriv(v3_, E, B, qm) : lorentz(v3_, E, B, qm);
+        V3 r4 = r + dt * v3_, v4 = w + dt * k3v;
+        fields_at<RF>(c, r4, t + dt, E, B);
+        V3 k4v = REL ? rk4_rel_deriv(v4, E, B, qm) : lorentz(v4, E, B, qm);
+        const double s6 = dt / 6.0;
+        r = r + s6 * (k1r + 2.0 * v2 + 2.0 * v3_ + v4);
+        w = w + s6 * (k1v + 2.0 * k2v + 2.0 * k3v + k4v);
+        if (REL) w = clamp_speed(w);
+    } else if constexpr (ALG == PPT_ALG_YOSHIDA || ALG == PPT_ALG_YOSHIDA_REL) {
+        constexpr bool REL = ALG == PPT_ALG_YOSHIDA_REL;
+        V3 E, B;
+        fields_at<RF>(c, r, t, E, B);
+        const double cs[3] = {kYoC1, kYoC2, kYoC1};
+        const double ds[3] = {kYoD1, kYoD2, kYoD1};
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            V3 a = REL ? rk4_rel_deriv(w, E, B, qm) : lorentz(w, E, B, qm);
+            w = w + (cs[s] * dt) * a;
+            r = r + (ds[s] * dt) * w;
+        }
+        if (REL) w = clamp_speed(w);
+    } else {
+        V3 E, B;
+        fields_at<RF>(c, r, t, E, B);
+        if constexpr (ALG == PPT_ALG_LEAPFROG) {
+            w = w + lorentz(w, E, B, qm) * dt;
+            r = r + w * dt;
+        } else if constexpr (ALG == PPT_ALG_BORIS) {
+            w = boris_v(w, E, B, dt, qm);
+            r = r + w * dt;
+        } else if constexpr (ALG == PPT_ALG_VAY_REL) {
+            w = vay_rel_v(w, E, B, dt, qm);
+            r = r + w * dt;
+        } else if constexpr (ALG == PPT_ALG_BORIS_REL) {
+            w = boris_rel_u(w, E, B, dt, qm);
+            r = r + w_to_v<ALG>(w) * dt;
+        } else {  // PPT_ALG_VAY
+            w = vay_u(w, E, B, dt, qm);
+            r = r + w_to_v<ALG>(w) * dt;
+        }
+    }
+}
+
+__device__ __forceinline__ void write_row(double* hist, int64_t rec, int64_t n, int64_t row, V3 a) {
+    double* p = hist + (rec * n + row) * 3;
+    p[0] = a.x;
+    p[1] = a.y;
+    p[2] = a.z;
+}
+
+__device__ __forceinline__ void add_counters(unsigned long long* counters, unsigned hits, unsigned steps) {
+    unsigned long long h = hits, s = steps;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        h += __shfl_down_sync(0xffffffffu, h, o);
+        s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters, h);
+        atomicAdd(counters + 1, s);
+    }
+}
+
+template <int ALG, bool RF>
+__global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ TrackDev P) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool live = s < P.n;
+    unsigned steps_done = 0;
+    Ctx c{&P.F, P.dt, P.qm, P.omega, 0.0, 0u};
+    if (live) {
+        const int64_t n = P.n;
+        double* st = P.f64;
+        V3 r = v3(st[s], st[n + s], st[2 * n + s]);
+        V3 w = v3(st[3 * n + s], st[4 * n + s], st[5 * n + s]);
+        const int64_t row = P.order ? P.order[s] : s;
+        if (RF) c.phase = P.rf_phase[s];
+
+        if (P.flags & PPT_TRACK_INIT) {
+            if constexpr (alg_staggered(ALG)) {
+                V3 E, B;
+                fields_at<RF>(c, r, P.t0 + (double)P.step0 * P.dt, E, B);
+                w = half_kick<ALG>(w, E, B, -0.5 * P.dt, P.qm);
+            }
+            if (P.r_hist) {
+                write_row(P.r_hist, 0, n, row, r);
+                write_row(P.v_hist, 0, n, row, w_to_v<ALG>(w));
+            }
+        }
+        // steps until the next record: record after global step g when (g+1) % rec == 0
+        int64_t g = P.step0;
+        int64_t until = P.rec_every - 1 - (g % P.rec_every);
+        for (int64_t k = 0; k < P.nsteps; ++k, ++g) {
+            step<ALG, RF>(c, r, w, P.t0 + (double)g * P.dt);
+            if (until == 0) {
+                const int64_t rec = (g + 1) / P.rec_every;
+                if (P.r_hist && rec < P.n_rec) {
+                    write_row(P.r_hist, rec, n, row, r);
+                    write_row(P.v_hist, rec, n, row, w_to_v<ALG>(w));
+                }
+                until = P.rec_every - 1;
+            } else {
+                --until;
+            }
+        }
+        steps_done = (unsigned)P.nsteps;
+        if (P.flags & PPT_TRACK_FINAL) {
+            if constexpr (alg_staggered(ALG)) {
+                V3 E, B;
+                fields_at<RF>(c, r, P.t0 + (double)P.nsteps_total * P.dt, E, B);
+                w = half_kick<ALG>(w, E, B, 0.5 * P.dt, P.qm);
+                if (P.v_hist) write_row(P.v_hist, P.n_rec - 1, n, row, w_to_v<ALG>(w));
+            }
+        }
+        st[s] = r.x;
+        st[n + s] = r.y;
+        st[2 * n + s] = r.z;
+        st[3 * n + s] = w.x;
+        st[4 * n + s] = w.y;
+        st[5 * n + s] = w.z;
+        if (P.status) {
+            double sum = r.x + r.y + r.z + w.x + w.y + w.z;
+            if (!isfinite(sum)) atomicOr(P.status, PPT_STATUS_NONFINITE);
+        }
+    }
+    if (P.counters) add_counters(P.counters, c.hits, steps_done);
+}
+
+template <int ALG>
+static cudaError_t launch_alg(const TrackDev& P, bool rf, cudaStream_t s) {
+    const int block = pick_block(P.n);
+    const int grid = grid_for(P.n, block);
+    if (rf) track_f64_kernel<ALG, true><<<grid, block, 0, s>>>(P);
+    else track_f64_kernel<ALG, false><<<grid, block, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+int launch_track_f64(const TrackDev& P, int algorithm, bool rf, cudaStream_t s) {
+    cudaError_t e;
+    switch (algorithm) {
+        case PPT_ALG_LEAPFROG: e = launch_alg<PPT_ALG_LEAPFROG>(P, rf, s); break;
+        case PPT_ALG_BORIS: e = launch_alg<PPT_ALG_BORIS>(P, rf, s); break;
+        case PPT_ALG_RK4: e = launch_alg<PPT_ALG_RK4>(P, rf, s); break;
+        case PPT_ALG_YOSHIDA: e = launch_alg<PPT_ALG_YOSHIDA>(P, rf, s); break;
+        case PPT_ALG_VAY_REL: e = launch_alg<PPT_ALG_VAY_REL>(P, rf, s); break;
+        case PPT_ALG_RK4_REL: e = launch_alg<PPT_ALG_RK4_REL>(P, rf, s); break;
+        case PPT_ALG_YOSHIDA_REL: e = launch_alg<PPT_ALG_YOSHIDA_REL>(P, rf, s); break;
+        case PPT_ALG_BORIS_REL: e = launch_alg<PPT_ALG_BORIS_REL>(P, rf, s); break;
+        case PPT_ALG_VAY: e = launch_alg<PPT_ALG_VAY>(P, rf, s); break;
+        default: return fail(PPT_ERR_ARG, "unknown algorithm");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "track_f64_kernel launch");
+    return PPT_OK;
+}
+
+}  // namespace ppt

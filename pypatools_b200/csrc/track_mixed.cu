@@ -1,0 +1,395 @@
+// Mixed-precision form of the fused push + trilinear gather.
+//
+// Same step structure and reference semantics as the float64 kernel
+// (Boris pusher.py:124-165, Vay 'vay_rel' :216-279, RK4 :803-892, leapfrog
+// :730-739, record indices :966-1007, fill 0 outside the map
+// interpolators.py:93-97), with:
+//   * positions as int32 cell + float32 in-cell offset (the offset is the
+//     trilinear weight: no per-step cell search),
+//   * float32 node records (128-bit loads), float32 interpolation and
+//     float32 rotation, computing the velocity INCREMENT of the step,
+//   * velocity state as a float32 hi/lo pair updated by an error-free sum,
+//   * float64 only for the field time t_n = t0 + n dt and the RF phase
+//     omega t + phi, reduced to [-pi, pi] before the float32 cosine.
+#include <cmath>
+
+#include "track_params.cuh"
+
+namespace ppt {
+
+
+constexpr double kTwoPi = 6.283185307179586;
+constexpr double kInvTwoPi = 0.15915494309189535;
+
+struct MixCtx {
+    const TrackMixDev* P;
+    double phase;
+    unsigned hits;
+};
+
+// Trilinear E/B at (cell, offset) from the float32 map; returns false when
+// outside (fields = the constant parts only).
+__device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3], F3& E,
+                                             F3& B) {
+    E = f3(P.e_const[0], P.e_const[1], P.e_const[2]);
+    B = f3(P.b_const[0], P.b_const[1], P.b_const[2]);
+    int i, j, k;
+    float tx, ty, tz;
+    if (!mixed_axis(cell[0], f[0], P.G.n[0], i, tx)) return false;
+    if (!mixed_axis(cell[1], f[1], P.G.n[1], j, ty)) return false;
+    if (!mixed_axis(cell[2], f[2], P.G.n[2], k, tz)) return false;
+    const MapDev& m = P.map;
+    const float* base = static_cast<const float*>(m.data) + ((int64_t)i * m.sx + (int64_t)j * m.sy + k) * m.stride;
+    const int64_t ox = m.sx * m.stride, oy = m.sy * m.stride, oz = m.stride;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        if (h == 0 && !m.has_e) continue;
+        if (h == 1 && !m.has_b) continue;
+        const float* b = base + (h == 0 ? 0 : m.b_off);
+        float4 q[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
+            q[c] = __ldg(reinterpret_cast<const float4*>(b + di * ox + dj * oy + dk * oz));
+        }
+        // x first, then y, then z (interpolators.py:127-135)
+        F3 o;
+        {
+            float c00 = lerp_f(q[0].x, q[4].x, tx), c01 = lerp_f(q[1].x, q[5].x, tx);
+            float c10 = lerp_f(q[2].x, q[6].x, tx), c11 = lerp_f(q[3].x, q[7].x, tx);
+            o.x = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
+        }
+        {
+            float c00 = lerp_f(q[0].y, q[4].y, tx), c01 = lerp_f(q[1].y, q[5].y, tx);
+            float c10 = lerp_f(q[2].y, q[6].y, tx), c11 = lerp_f(q[3].y, q[7].y, tx);
+            o.y = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
+        }
+        {
+            float c00 = lerp_f(q[0].z, q[4].z, tx), c01 = lerp_f(q[1].z, q[5].z, tx);
+            float c10 = lerp_f(q[2].z, q[6].z, tx), c11 = lerp_f(q[3].z, q[7].z, tx);
+            o.z = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
+        }
+        if (h == 0) E = E + o; else B = B + o;
+    }
+    return true;
+}
+
+template <bool RF>
+__device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], double t, F3& E,
+                                             F3& B) {
+    bool in = gather_mixed(*c.P, cell, f, E, B);
+    c.hits += in;
+    if (RF) {
+        if (E.x != 0.0f || E.y != 0.0f || E.z != 0.0f) {
+            double ph = c.P->omega * t + c.phase;
+            double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
+            float cf = cosf((float)red);
+            E = cf * E;
+        }
+    }
+    return in || c.P->const_nz;
+}
+
+// Boris velocity increment in float32 (pusher.py:149-163 rearranged):
+// v_new - v = 2 a + (v- + v- x t) x s,  a = (q/m) E dt/2,  v- = v + a.
+__device__ __forceinline__ F3 boris_dv(F3 v, F3 E, F3 B, float hqdt) {
+    F3 a = hqdt * E;
+    F3 vm = v + a;
+    F3 t = hqdt * B;
+    float s_f = __fdividef(2.0f, 1.0f + dotf(t, t));
+    F3 s = s_f * t;
+    F3 vp = vm + crossf(vm, t);
+    F3 c2 = crossf(vp, s);
+    return f3(fmaf(2.0f, a.x, c2.x), fmaf(2.0f, a.y, c2.y), fmaf(2.0f, a.z, c2.z));
+}
+
+constexpr float kCf = 299792458.0f;
+
+__device__ __forceinline__ float rel_gamma_f(F3 v) {
+    float bsq = dotf(v, v) * (1.0f / (kCf * kCf));
+    bsq = bsq >= 0.9999f ? 0.9999f : bsq;
+    return rsqrtf(1.0f - bsq);
+}
+
+__device__ __forceinline__ F3 lorentz_f(F3 v, F3 E, F3 B, float qm) { return qm * (E + crossf(v, B)); }
+
+__device__ __forceinline__ F3 rk4_rel_deriv_f(F3 v, F3 E, F3 B, float qm) {
+    float g = rel_gamma_f(v);
+    F3 F = qm * (E + crossf(v, B));
+    float ig = 1.0f / g;
+    float k = dotf(v, F) * ig * (1.0f / (kCf * kCf));
+    return f3(fmaf(F.x, ig, -k * v.x), fmaf(F.y, ig, -k * v.y), fmaf(F.z, ig, -k * v.z));
+}
+
+// pusher.py:216-279 in float32; returns the new velocity (not an increment).
+__device__ __forceinline__ F3 vay_rel_f(F3 v, F3 E, F3 B, float qm, float dt) {
+    float g = rel_gamma_f(v);
+    F3 u = g * v;
+    F3 tau = (0.5f * qm * dt) * B;
+    F3 up = u + (qm * dt) * E;
+    float upm2 = dotf(up, up);
+    float tau2 = dotf(tau, tau);
+    float udt = dotf(up, tau);
+    float gis = 1.0f - upm2 * (1.0f / (kCf * kCf));
+    gis = gis < 1e-10f ? 1e-10f : gis;
+    float sigma = gis - tau2;
+    float q = udt * (1.0f / kCf);
+    float gn = sqrtf(0.5f * (sigma + sqrtf(fmaf(sigma, sigma, 4.0f * (tau2 + q * q)))));
+    float ig = 1.0f / gn;
+    F3 t = ig * tau;
+    float sf = 2.0f / (1.0f + tau2 * ig * ig);
+    F3 s = sf * t;
+    F3 us = up + crossf(up, t);
+    F3 un = up + crossf(us, s);
+    F3 vn = ig * un;
+    float vm = sqrtf(dotf(vn, vn));
+    if (vm >= 0.9999f * kCf) vn = ((0.9999f * kCf) / vm) * vn;
+    return vn;
+}
+
+__device__ __forceinline__ void vel_add(float vh[3], float vl[3], F3 d) {
+    ff_add(vh[0], vl[0], d.x);
+    ff_add(vh[1], vl[1], d.y);
+    ff_add(vh[2], vl[2], d.z);
+}
+
+__device__ __forceinline__ void vel_set(float vh[3], float vl[3], F3 v) {
+    // replace the state by a float32 value (clamped / recomputed velocity)
+    vh[0] = v.x; vh[1] = v.y; vh[2] = v.z;
+    vl[0] = vl[1] = vl[2] = 0.0f;
+}
+
+__device__ __forceinline__ void advance(const TrackMixDev& P, int cell[3], float f[3], const float vh[3],
+                                        const float vl[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) advance_axis(cell[a], f[a], vh[a], vl[a], P.kh[a], P.kl[a]);
+}
+
+// Cell + offset of the point (cell, f) + d (d in metres), for RK4 stages.
+__device__ __forceinline__ void offset_point(const TrackMixDev& P, const int cell[3], const float f[3], F3 d,
+                                             int oc[3], float of[3]) {
+    const float dd[3] = {d.x, d.y, d.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float g = fmaf(dd[a], P.inv_d[a], f[a]);
+        float c = floorf(g);
+        of[a] = g - c;
+        oc[a] = cell[a] + (int)c;
+        if (of[a] >= 1.0f) { of[a] -= 1.0f; oc[a] += 1; }
+    }
+}
+
+template <int ALG, bool RF>
+__device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float vh[3], float vl[3],
+                                           double t) {
+    const TrackMixDev& P = *c.P;
+    F3 v = f3(vh[0], vh[1], vh[2]);
+    if constexpr (ALG == PPT_ALG_BORIS) {
+        F3 E, B;
+        if (fields_mixed<RF>(c, cell, f, t, E, B)) vel_add(vh, vl, boris_dv(v, E, B, P.hqdt));
+        advance(P, cell, f, vh, vl);
+    } else if constexpr (ALG == PPT_ALG_LEAPFROG) {
+        F3 E, B;
+        if (fields_mixed<RF>(c, cell, f, t, E, B)) vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
+        advance(P, cell, f, vh, vl);
+    } else if constexpr (ALG == PPT_ALG_VAY_REL) {
+        F3 E, B;
+        fields_mixed<RF>(c, cell, f, t, E, B);
+        F3 vn = vay_rel_f(v, E, B, P.qm, P.dtf);
+        // increment relative to the float32 head keeps the low part's bits
+        vel_add(vh, vl, vn - v);
+        advance(P, cell, f, vh, vl);
+    } else {  // RK4 / RK4_REL (pusher.py:803-892), stage times t, t+h, t+h, t+dt
+        constexpr bool REL = ALG == PPT_ALG_RK4_REL;
+        const float dt = P.dtf, h = 0.5f * dt;
+        F3 E, B;
+        int sc[3];
+        float sf[3];
+        fields_mixed<RF>(c, cell, f, t, E, B);
+        F3 k1 = REL ? rk4_rel_deriv_f(v, E, B, P.qm) : lorentz_f(v, E, B, P.qm);
+        F3 v2 = v + h * k1;
+        offset_point(P, cell, f, h * v, sc, sf);
+        fields_mixed<RF>(c, sc, sf, t + 0.5 * P.dt, E, B);
+        F3 k2 = REL ? rk4_rel_deriv_f(v2, E, B, P.qm) : lorentz_f(v2, E, B, P.qm);
+        F3 v3_ = v + h * k2;
+        offset_point(P, cell, f, h * v2, sc, sf);
+        fields_mixed<RF>(c, sc, sf, t + 0.5 * P.dt, E, B);
+        F3 k3 = REL ? rk4_rel_deriv_f(v3_, E, B, P.qm) : lorentz_f(v3_, E, B, P.qm);
+        F3 v4 = v + dt * k3;
+        offset_point(P, cell, f, dt * v3_, sc, sf);
+        fields_mixed<RF>(c, sc, sf, t + P.dt, E, B);
+        F3 k4 = REL ? rk4_rel_deriv_f(v4, E, B, P.qm) : lorentz_f(v4, E, B, P.qm);
+        // r_new - r = dt v + dt^2/6 (k1 + k2 + k3); v_new - v = dt/6 (k1 + 2k2 + 2k3 + k4)
+        const float s6 = dt * (1.0f / 6.0f);
+        F3 dr = (dt * s6) * (k1 + k2 + k3);
+        F3 dv = s6 * (k1 + 2.0f * k2 + 2.0f * k3 + k4);
+        const float drv[3] = {dr.x, dr.y, dr.z};
+        // position: the dt v part in float-float, the stage correction in float32
+        advance(P, cell, f, vh, vl);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float g = fmaf(drv[a], P.inv_d[a], f[a]);
+            float cc = floorf(g);
+            f[a] = g - cc;
+            cell[a] += (int)cc;
+            if (f[a] >= 1.0f) { f[a] -= 1.0f; cell[a] += 1; }
+        }
+        vel_add(vh, vl, dv);
+        if (REL) {
+            F3 vn = f3(vh[0], vh[1], vh[2]);
+            float vm = sqrtf(dotf(vn, vn));
+            if (vm >= 0.9999f * kCf) vel_set(vh, vl, ((0.9999f * kCf) / vm) * vn);
+        }
+    }
+}
+
+__device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t rec, int64_t row, const int cell[3],
+                                                const float f[3], const float vh[3], const float vl[3],
+                                                bool r_too) {
+    const int64_t o = (rec * P.n + row) * 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (r_too) P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + (double)f[a]) * P.G.d[a];
+        P.v_hist[o + a] = (double)vh[a] + (double)vl[a];
+    }
+}
+
+template <int ALG, bool RF>
+__global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool live = s < P.n;
+    unsigned steps_done = 0;
+    MixCtx c{&P, 0.0, 0u};
+    if (live) {
+        const int64_t n = P.n;
+        int cell[3];
+        float f[3], vh[3], vl[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            cell[a] = P.ci[a * n + s];
+            f[a] = P.fs[a * n + s];
+            vh[a] = P.fs[(3 + a) * n + s];
+            vl[a] = P.fs[(6 + a) * n + s];
+        }
+        const int64_t row = P.order ? P.order[s] : s;
+        if (RF) c.phase = P.rf_phase[s];
+        if (P.flags & PPT_TRACK_INIT) {
+            if constexpr (ALG == PPT_ALG_BORIS) {
+                F3 E, B;
+                if (fields_mixed<RF>(c, cell, f, P.t0 + (double)P.step0 * P.dt, E, B))
+                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -P.hqdt));
+            }
+            if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
+        }
+        int64_t g = P.step0;
+        int64_t until = P.rec_every - 1 - (g % P.rec_every);
+        for (int64_t k = 0; k < P.nsteps; ++k, ++g) {
+            mixed_step<ALG, RF>(c, cell, f, vh, vl, P.t0 + (double)g * P.dt);
+            if (until == 0) {
+                const int64_t rec = (g + 1) / P.rec_every;
+                if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, vh, vl, true);
+                until = P.rec_every - 1;
+            } else {
+                --until;
+            }
+        }
+        steps_done = (unsigned)P.nsteps;
+        if (P.flags & PPT_TRACK_FINAL) {
+            if constexpr (ALG == PPT_ALG_BORIS) {
+                F3 E, B;
+                if (fields_mixed<RF>(c, cell, f, P.t0 + (double)P.nsteps_total * P.dt, E, B))
+                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, P.hqdt));
+                if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            P.ci[a * n + s] = cell[a];
+            P.fs[a * n + s] = f[a];
+            P.fs[(3 + a) * n + s] = vh[a];
+            P.fs[(6 + a) * n + s] = vl[a];
+        }
+        if (P.status) {
+            float sum = f[0] + f[1] + f[2] + vh[0] + vh[1] + vh[2];
+            if (!isfinite(sum)) atomicOr(P.status, PPT_STATUS_NONFINITE);
+        }
+    }
+    if (P.counters) {
+        unsigned long long h = c.hits, st = steps_done;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            h += __shfl_down_sync(0xffffffffu, h, o);
+            st += __shfl_down_sync(0xffffffffu, st, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(P.counters, h);
+            atomicAdd(P.counters + 1, st);
+        }
+    }
+}
+
+template <int ALG>
+static cudaError_t launch_mixed_alg(const TrackMixDev& P, bool rf, cudaStream_t s) {
+    const int block = pick_block(P.n);
+    const int grid = grid_for(P.n, block);
+    if (rf) track_mixed_kernel<ALG, true><<<grid, block, 0, s>>>(P);
+    else track_mixed_kernel<ALG, false><<<grid, block, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s) {
+    cudaError_t e;
+    switch (algorithm) {
+        case PPT_ALG_LEAPFROG: e = launch_mixed_alg<PPT_ALG_LEAPFROG>(P, rf, s); break;
+        case PPT_ALG_BORIS: e = launch_mixed_alg<PPT_ALG_BORIS>(P, rf, s); break;
+        case PPT_ALG_RK4: e = launch_mixed_alg<PPT_ALG_RK4>(P, rf, s); break;
+        case PPT_ALG_VAY_REL: e = launch_mixed_alg<PPT_ALG_VAY_REL>(P, rf, s); break;
+        case PPT_ALG_RK4_REL: e = launch_mixed_alg<PPT_ALG_RK4_REL>(P, rf, s); break;
+        default:
+            return fail(PPT_ERR_UNSUPPORTED,
+                        "the mixed form covers leapfrog, boris, rk4, vay_rel and rk4_rel; use precision 'fp64'");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "track_mixed_kernel launch");
+    return PPT_OK;
+}
+
+// host-side construction of the mixed kernel parameters
+int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_args* a, int64_t n_rec,
+                     TrackMixDev* P) {
+    int rc = mixed_grid(F, &P->G);
+    if (rc) return rc;
+    P->map = F.maps[0];
+    for (int c = 0; c < 3; ++c) {
+        P->e_const[c] = (float)F.e_const[c];
+        P->b_const[c] = (float)F.b_const[c];
+        double k = a->dt / P->G.d[c];
+        P->kh[c] = (float)k;
+        P->kl[c] = (float)(k - (double)P->kh[c]);
+        P->inv_d[c] = (float)P->G.inv_d[c];
+    }
+    P->const_nz = F.e_const_nz || F.b_const_nz;
+    P->n = st->n;
+    P->step0 = a->step0;
+    P->nsteps = a->nsteps;
+    P->nsteps_total = a->nsteps_total;
+    P->rec_every = a->rec_every;
+    P->n_rec = n_rec;
+    P->flags = a->flags;
+    P->dt = a->dt;
+    P->t0 = a->t0;
+    P->omega = a->rf_omega;
+    P->qm = (float)a->q_over_m;
+    P->hqdt = (float)(0.5 * a->q_over_m * a->dt);
+    P->dtf = (float)a->dt;
+    P->rf_phase = a->rf_phase;
+    P->ci = st->i32;
+    P->fs = st->f32;
+    P->r_hist = a->r_hist;
+    P->v_hist = a->v_hist;
+    P->order = a->order;
+    P->status = a->status;
+    P->counters = a->counters;
+    return PPT_OK;
+}
+
+}  // namespace ppt

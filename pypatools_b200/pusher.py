@@ -1,0 +1,383 @@
+"""GPU drop-in for the reference's ``Pusher`` (src/PyPATools/pusher.py:430-1037).
+
+``PusherGPU`` keeps the reference's constructor, method names, signatures,
+return shapes and error messages:
+
+    Pusher(ion, algorithm='boris', use_numba=True, electrode_assembly=None)
+    push(r(3,), v(3,), efield, bfield, dt)                      -> (r, v)
+    track(r0(3,), v0(3,), efield, bfield, nsteps, dt, rec_every_n_steps=1)
+                                                                -> (r_hist(n_rec,3), v_hist)
+    push_batch(r(M,3), v(M,3), efield, bfield, dt)              -> (r, v)
+    track_batch(r0(M,3), v0(M,3), efield, bfield, nsteps, dt, rec_every_n_steps=1, verbose=False)
+                                                                -> (r_hist(n_rec,M,3), v_hist, active(M,))
+    change_algorithm(name), ALGORITHMS, __repr__
+
+and adds keyword-only options: ``precision`` ('fp64' = the reference method
+in float64, the drop-in; 'mixed' = the mixed-precision form), ``device``,
+``snapshot`` ('host' numpy arrays like the reference, or 'device' torch
+tensors), ``steps_per_launch``, ``sort_every`` (cell re-sort interval) and,
+on ``track_batch``, ``rf`` (an ``RFModulation`` multiplying E by
+cos(2 pi f t + phi_i)) and ``t0``.
+
+All work runs in libppt.so kernels; there is no CPU fallback.
+"""
+import math
+import warnings
+
+import numpy as np
+
+from . import _lib
+from .device_fields import FieldCache
+
+REFERENCE_ALGORITHMS = ["leapfrog", "boris", "rk4", "yoshida", "vay_rel", "rk4_rel", "yoshida_rel"]
+EXTRA_ALGORITHMS = ["boris_rel", "vay"]
+MIXED_ALGORITHMS = ("leapfrog", "boris", "rk4", "vay_rel", "rk4_rel")
+
+
+class RFModulation:
+    """Time dependence of E: E(x, t) = E(x) cos(2 pi frequency t + phase_i).
+
+    ``phase`` is a scalar or one value per particle [rad]."""
+
+    def __init__(self, frequency, phase=0.0):
+        self.frequency = float(frequency)
+        self.phase = phase
+
+    @property
+    def omega(self):
+        return 2.0 * math.pi * self.frequency
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("PusherGPU needs a CUDA device (there is no CPU fallback)")
+    return torch
+
+
+def default_steps_per_launch(n, nsteps):
+    """Steps per kernel launch: whole tracks for small bunches, about 4e9
+    particle-steps per launch for large ones (launches of roughly a second or
+    less, so the stream stays responsive)."""
+    if nsteps <= 0:
+        return 1
+    return int(max(1, min(nsteps, 2 ** 31 - 1, math.ceil(4e9 / max(n, 1)))))
+
+
+class DeviceTracker:
+    """Device-resident state of one bunch: the building block of
+    ``track_batch``, the serving loop and the benchmark.
+
+    State (structure of arrays), snapshot histories, the slot -> row order
+    after cell sorts, the RF phases and the device status word all live in
+    torch CUDA tensors owned by this object."""
+
+    def __init__(self, algorithm, q_over_m, dfields, n, nsteps_total, dt, rec_every=1, precision="fp64",
+                 rf_omega=0.0, rf_phase=None, t0=0.0, record=True, stagger=True, counters=False,
+                 device=None):
+        torch = _torch()
+        self.torch = torch
+        if algorithm not in _lib.ALG_IDS:
+            raise ValueError(f"unknown algorithm {algorithm!r}")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if precision == "mixed" and algorithm not in MIXED_ALGORITHMS:
+            raise NotImplementedError(f"the mixed form covers {MIXED_ALGORITHMS}; use precision='fp64'")
+        if rec_every < 1:
+            raise ValueError("rec_every_n_steps must be >= 1")
+        self.lib = _lib.load()
+        self.device = torch.device(device) if device is not None else dfields.device
+        self.algorithm = algorithm
+        self.precision = precision
+        self.q_over_m = float(q_over_m)
+        self.dfields = dfields
+        self.n = int(n)
+        self.nsteps_total = int(nsteps_total)
+        self.dt = float(dt)
+        self.rec_every = int(rec_every)
+        self.n_rec = self.nsteps_total // self.rec_every + 1
+        self.t0 = float(t0)
+        self.stagger = stagger
+        self.step = 0
+        dev = self.device
+        n = self.n
+        if precision == "fp64":
+            self.f64 = torch.empty(6 * n, dtype=torch.float64, device=dev)
+            self.i32 = self.f32 = None
+        else:
+            self.f64 = None
+            self.i32 = torch.empty(3 * n, dtype=torch.int32, device=dev)
+            self.f32 = torch.empty(9 * n, dtype=torch.float32, device=dev)
+        self.state = _lib.State(_lib.PREC_F64 if precision == "fp64" else _lib.PREC_MIXED,
+                                _lib.ALG_IDS[algorithm], n,
+                                self.f64.data_ptr() if self.f64 is not None else None,
+                                self.i32.data_ptr() if self.i32 is not None else None,
+                                self.f32.data_ptr() if self.f32 is not None else None)
+        if record:
+            self.r_hist = torch.empty((self.n_rec, n, 3), dtype=torch.float64, device=dev)
+            self.v_hist = torch.empty((self.n_rec, n, 3), dtype=torch.float64, device=dev)
+        else:
+            self.r_hist = self.v_hist = None
+        self.rf_omega = float(rf_omega)
+        if rf_phase is not None:
+            ph = torch.as_tensor(rf_phase, dtype=torch.float64)
+            if ph.ndim == 0:
+                ph = ph.expand(n)
+            self.rf_phase = ph.to(dev).contiguous().clone()
+        else:
+            self.rf_phase = None
+        self.order = None
+        self.sort_scratch = None
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.counters = torch.zeros(2, dtype=torch.int64, device=dev) if counters else None
+        self.launches = 0
+
+    def _stream(self, stream):
+        return _lib.stream_handle(stream)
+
+    def load(self, r, v, stream=None):
+        """r, v: (n,3) float64 CUDA tensors."""
+        _lib.check(self.lib.ppt_state_load(self.state, self.dfields.fields, r.data_ptr(), v.data_ptr(),
+                                           self._stream(stream)))
+        self.launches += 1
+
+    def advance(self, k, stream=None):
+        k = int(k)
+        if self.step + k > self.nsteps_total:
+            raise ValueError("advance past nsteps_total")
+        flags = 0
+        if self.stagger:
+            if self.step == 0:
+                flags |= _lib.TRACK_INIT
+            if self.step + k == self.nsteps_total:
+                flags |= _lib.TRACK_FINAL
+        a = _lib.TrackArgs()
+        a.step0 = self.step
+        a.nsteps = k
+        a.nsteps_total = self.nsteps_total
+        a.rec_every = self.rec_every
+        a.flags = flags
+        a.dt = self.dt
+        a.q_over_m = self.q_over_m
+        a.t0 = self.t0
+        a.rf_omega = self.rf_omega
+        a.rf_phase = self.rf_phase.data_ptr() if self.rf_phase is not None else None
+        a.r_hist = self.r_hist.data_ptr() if self.r_hist is not None else None
+        a.v_hist = self.v_hist.data_ptr() if self.v_hist is not None else None
+        a.order = self.order.data_ptr() if self.order is not None else None
+        a.status = self.status.data_ptr()
+        a.counters = self.counters.data_ptr() if self.counters is not None else None
+        _lib.check(self.lib.ppt_track(self.state, self.dfields.fields, a, self._stream(stream)))
+        if k > 0 or flags:
+            self.launches += 1
+        self.step += k
+
+    def sort(self, stream=None):
+        """Reorder particles by cell (gather locality)."""
+        torch = self.torch
+        if not self.dfields.has_maps or self.n == 0:
+            return
+        if self.order is None:
+            self.order = torch.arange(self.n, dtype=torch.int64, device=self.device)
+        if self.sort_scratch is None:
+            nbytes = self.lib.ppt_cell_sort_scratch_bytes(self.n)
+            self.sort_scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        _lib.check(self.lib.ppt_cell_sort(self.state, self.dfields.fields, self.order.data_ptr(),
+                                          self.rf_phase.data_ptr() if self.rf_phase is not None else None,
+                                          self.sort_scratch.data_ptr(), self._stream(stream)))
+        self.launches += 1
+
+    def store(self, r, v, stream=None):
+        """Write the current state as (n,3) float64 r, v in row order."""
+        _lib.check(self.lib.ppt_state_store(self.state, self.dfields.fields,
+                                            self.order.data_ptr() if self.order is not None else None,
+                                            r.data_ptr() if r is not None else None,
+                                            v.data_ptr() if v is not None else None, self._stream(stream)))
+        self.launches += 1
+
+    def device_status(self):
+        return int(self.status.item())
+
+    def counter_values(self):
+        if self.counters is None:
+            return None
+        c = self.counters.cpu().numpy()
+        return {"map_hits": int(c[0]), "particle_steps": int(c[1])}
+
+
+class PusherGPU:
+    """Batch and single-particle tracking on the GPU with the reference's API."""
+
+    ALGORITHMS = list(REFERENCE_ALGORITHMS)
+    EXTRA_ALGORITHMS = list(EXTRA_ALGORITHMS)
+
+    def __init__(self, ion, algorithm="boris", use_numba=True, electrode_assembly=None, *, precision="fp64",
+                 device=None, snapshot="host", steps_per_launch=None, sort_every=0):
+        self.ion = ion
+        self.q_over_m = ion.q_over_m
+        algorithm = algorithm.lower()
+        if algorithm not in self.ALGORITHMS + self.EXTRA_ALGORITHMS:
+            raise ValueError(f"Unknown algorithm '{algorithm}'. Must be one of {self.ALGORITHMS}")
+        # pusher.py:482-489: leapfrog with a >100 keV ion object switches to vay_rel
+        if algorithm == "leapfrog" and hasattr(ion, "energy_mev") and ion.energy_mev > 0.1:
+            warnings.warn("Leapfrog is non-relativistic. Using 'vay_rel' instead for better relativistic "
+                          "accuracy.", UserWarning)
+            algorithm = "vay_rel"
+        if electrode_assembly:
+            raise NotImplementedError("electrode collision termination is not on the GPU path; "
+                                      "track without an electrode assembly")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if snapshot not in ("host", "device"):
+            raise ValueError("snapshot must be 'host' or 'device'")
+        self.algorithm = algorithm
+        self.use_numba = use_numba
+        self.relativistic = algorithm.endswith("_rel")
+        self.elec_assy = electrode_assembly
+        self.precision = precision
+        self.device = device
+        self.snapshot = snapshot
+        self.steps_per_launch = steps_per_launch
+        self.sort_every = int(sort_every)
+        self._fields = FieldCache(capacity=4)
+        self.last_tracker = None
+
+    # -- helpers -----------------------------------------------------------
+    def _device_fields(self, efield, bfield):
+        _torch()
+        return self._fields.get(efield, bfield, self.precision, self.device)
+
+    @staticmethod
+    def _as_rows(a, name):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        if a.ndim != 2 or a.shape[1] != 3:
+            raise ValueError(f"{name} must have shape (M, 3), got {a.shape}")
+        return a
+
+    def _upload(self, a, device):
+        torch = _torch()
+        t = torch.from_numpy(a)
+        if device.type == "cuda":
+            t = t.pin_memory()
+        return t.to(device, non_blocking=True)
+
+    # -- batch API -----------------------------------------------------------
+    def push_batch(self, r_array, v_array, efield, bfield, dt):
+        """One step for M particles (pusher.py:699-801): no half-step
+        staggering, exactly the reference's push_batch."""
+        if not np.isscalar(dt):
+            raise TypeError("dt must be a scalar on the GPU path")
+        r = self._as_rows(r_array, "r_array")
+        v = self._as_rows(v_array, "v_array")
+        if r.shape != v.shape:
+            raise ValueError("r_array and v_array must have the same shape")
+        m = r.shape[0]
+        if m == 0:
+            return r.copy(), v.copy()
+        torch = _torch()
+        df = self._device_fields(efield, bfield)
+        tr = DeviceTracker(self.algorithm, self.q_over_m, df, m, 1, dt, 1, self.precision, record=False,
+                           stagger=False, device=self.device)
+        d_r, d_v = self._upload(r, df.device), self._upload(v, df.device)
+        with torch.cuda.device(df.device):
+            tr.load(d_r, d_v)
+            tr.advance(1)
+            tr.store(d_r, d_v)
+        return d_r.cpu().numpy(), d_v.cpu().numpy()
+
+    def track_batch(self, r0_array, v0_array, efield, bfield, nsteps, dt, rec_every_n_steps=1, verbose=False,
+                    *, rf=None, t0=0.0):
+        """Track M particles (pusher.py:894-1012).  Returns
+        (r_hist (n_rec, M, 3), v_hist, active (M,)) with
+        n_rec = nsteps // rec_every_n_steps + 1."""
+        if not np.isscalar(dt):
+            raise TypeError("dt must be a scalar on the GPU path")
+        nsteps = int(nsteps)
+        rec = int(rec_every_n_steps)
+        if nsteps < 0:
+            raise ValueError("nsteps must be >= 0")
+        if rec < 1:
+            raise ValueError("rec_every_n_steps must be >= 1")
+        r0 = self._as_rows(r0_array, "r0_array")
+        v0 = self._as_rows(v0_array, "v0_array")
+        if r0.shape != v0.shape:
+            raise ValueError("r0_array and v0_array must have the same shape")
+        m = r0.shape[0]
+        n_rec = nsteps // rec + 1
+        torch = _torch()
+        if m == 0:
+            empty = np.full((n_rec, 0, 3), np.nan)
+            if self.snapshot == "device":
+                return (torch.from_numpy(empty).cuda(), torch.from_numpy(empty.copy()).cuda(),
+                        np.ones(0, dtype=bool))
+            return empty, empty.copy(), np.ones(0, dtype=bool)
+        df = self._device_fields(efield, bfield)
+        rf_omega, rf_phase = 0.0, None
+        if rf is not None:
+            rf_omega = rf.omega
+            rf_phase = np.broadcast_to(np.asarray(rf.phase, dtype=np.float64), (m,))
+            rf_phase = torch.from_numpy(np.ascontiguousarray(rf_phase))
+        tr = DeviceTracker(self.algorithm, self.q_over_m, df, m, nsteps, dt, rec, self.precision,
+                           rf_omega=rf_omega, rf_phase=rf_phase, t0=t0, record=True, device=self.device)
+        self.last_tracker = tr
+        chunk = self.steps_per_launch or default_steps_per_launch(m, nsteps)
+        if self.sort_every > 0:
+            chunk = min(chunk, self.sort_every)
+        with torch.cuda.device(df.device):
+            tr.load(self._upload(r0, df.device), self._upload(v0, df.device))
+            done = 0
+            if nsteps == 0:
+                tr.advance(0)
+            while done < nsteps:
+                if self.sort_every > 0 and done > 0 and done % self.sort_every == 0:
+                    tr.sort()
+                k = min(chunk, nsteps - done)
+                if verbose:
+                    print(f"Step {done}/{nsteps} ({100 * done / nsteps:.0f}%)")
+                tr.advance(k)
+                done += k
+            status = tr.device_status()
+        if status & _lib.STATUS_NONFINITE:
+            warnings.warn("non-finite particle state encountered during tracking", RuntimeWarning)
+        if verbose:
+            print(f"Tracking complete: {nsteps} steps, {m} particles")
+        active = np.ones(m, dtype=bool)
+        if self.snapshot == "device":
+            return tr.r_hist, tr.v_hist, active
+        return tr.r_hist.cpu().numpy(), tr.v_hist.cpu().numpy(), active
+
+    # -- single-particle API -------------------------------------------------
+    def push(self, r, v, efield, bfield, dt):
+        """One step of one particle (pusher.py:508-565)."""
+        rn, vn = self.push_batch(np.asarray(r, dtype=np.float64).reshape(1, 3),
+                                 np.asarray(v, dtype=np.float64).reshape(1, 3), efield, bfield, dt)
+        return rn[0], vn[0]
+
+    def track(self, r0, v0, efield, bfield, nsteps, dt, rec_every_n_steps=1):
+        """Track one particle (pusher.py:620-693): (n_rec, 3) histories."""
+        snap = self.snapshot
+        self.snapshot = "host"
+        try:
+            rh, vh, _ = self.track_batch(np.asarray(r0, dtype=np.float64).reshape(1, 3),
+                                         np.asarray(v0, dtype=np.float64).reshape(1, 3), efield, bfield,
+                                         nsteps, dt, rec_every_n_steps)
+        finally:
+            self.snapshot = snap
+        return rh[:, 0, :], vh[:, 0, :]
+
+    # -- utilities -------------------------------------------------------------
+    def change_algorithm(self, algorithm):
+        algorithm = algorithm.lower()
+        if algorithm not in self.ALGORITHMS + self.EXTRA_ALGORITHMS:
+            raise ValueError(f"Unknown algorithm '{algorithm}'. Must be one of {self.ALGORITHMS}")
+        self.__init__(self.ion, algorithm=algorithm, use_numba=self.use_numba, precision=self.precision,
+                      device=self.device, snapshot=self.snapshot, steps_per_launch=self.steps_per_launch,
+                      sort_every=self.sort_every)
+
+    def __repr__(self):
+        return (f"PusherGPU(ion={getattr(self.ion, 'name', '?')}, algorithm='{self.algorithm}', "
+                f"relativistic={self.relativistic}, precision={self.precision})")
+
+
+# The reference's class name, so scripts can switch with one import.
+Pusher = PusherGPU

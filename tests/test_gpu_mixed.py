@@ -1,0 +1,85 @@
+"""Mixed-precision form vs the float64 oracle.
+
+Error metric (per particle, max over the bunch and all records):
+|r - r_ref| / max(|r_ref|, half-width of the map) and |v - v_ref| / |v_ref|.
+Target: <= 1e-6 relative position error for the fused Boris push on the RF
+gap workload over its full 2e4 steps."""
+import numpy as np
+import pytest
+
+from oracle import pusher_oracle as orc
+from pypatools_b200 import PusherGPU, RFModulation, workloads
+from tests.helpers import rel_pos_err, rel_vel_err, gpu_fields, half_width
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_fields_sparse(wl):
+    """Oracle maps with all-zero components dropped (same values, less memory)."""
+    def clean(vals):
+        if vals is None:
+            return orc.ZeroField()
+        return orc.MapField(wl.grid, {c: (None if vals[c] is None or not np.any(vals[c]) else vals[c])
+                                      for c in "xyz"})
+    return clean(wl.e_values), clean(wl.b_values)
+
+
+def test_mixed_boris_rf_gap_full_length_vs_oracle(cuda):
+    wl = workloads.rf_gap_protons(n=256, nsteps=20000, rec_every=500)
+    e, b = gpu_fields(wl)
+    rf = RFModulation(wl.rf_frequency, wl.rf_phase)
+    rh, vh, _ = PusherGPU(wl.species, "boris", precision="mixed").track_batch(
+        wl.r0, wl.v0, e, b, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
+    oe, ob = _oracle_fields_sparse(wl)
+    ro, vo, _ = orc.track_batch("boris", wl.species.q_over_m, wl.r0, wl.v0, oe, ob, wl.nsteps, wl.dt,
+                                wl.rec_every, rf=(2 * np.pi * wl.rf_frequency, wl.rf_phase))
+    err_r = rel_pos_err(rh, ro, half_width(wl))
+    err_v = rel_vel_err(vh, vo)
+    print(f"mixed boris rf gap: max rel pos err {err_r:.3e}, vel {err_v:.3e}")
+    assert err_r <= 1e-6
+    assert err_v <= 1e-6
+
+
+def test_mixed_boris_matches_fp64_gpu_at_scale(cuda):
+    # 65536 particles, full length: mixed vs the (oracle-pinned) float64 GPU path
+    wl = workloads.rf_gap_protons(n=65536, nsteps=20000, rec_every=500)
+    e, b = gpu_fields(wl)
+    rf = RFModulation(wl.rf_frequency, wl.rf_phase)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        out[prec] = PusherGPU(wl.species, "boris", precision=prec, snapshot="device").track_batch(
+            wl.r0, wl.v0, e, b, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
+    rh = out["mixed"][0].cpu().numpy()
+    ro = out["fp64"][0].cpu().numpy()
+    err_r = rel_pos_err(rh, ro, half_width(wl))
+    print(f"mixed vs fp64 (65536 x 2e4): max rel pos err {err_r:.3e}")
+    assert err_r <= 1e-6
+
+
+def test_mixed_boris_quad_solenoid(cuda, golden):
+    wl = workloads.quad_solenoid_protons()
+    e, b = gpu_fields(wl)
+    rh, vh, _ = PusherGPU(wl.species, "boris", precision="mixed").track_batch(wl.r0, wl.v0, e, b, 1000, wl.dt, 500)
+    err_r = rel_pos_err(rh, golden["c1/boris/r_hist"], half_width(wl))
+    err_v = rel_vel_err(vh, golden["c1/boris/v_hist"])
+    print(f"mixed boris quad solenoid: pos {err_r:.3e} vel {err_v:.3e}")
+    # float32 map values (the reference's are float64) bound this at ~1e-7
+    assert err_r <= 1e-6 and err_v <= 1e-6
+
+
+@pytest.mark.parametrize("alg,bound", [("boris", 1e-5), ("vay_rel", 1e-3), ("rk4_rel", 1e-4)])
+def test_mixed_electron_sweep_error_report(cuda, golden, alg, bound):
+    wl = workloads.radial_e_solenoid_electrons(n=128)
+    e, b = gpu_fields(wl)
+    rh, vh, _ = PusherGPU(wl.species, alg, precision="mixed").track_batch(wl.r0, wl.v0, e, b, 10000, wl.dt, 2500)
+    err_r = rel_pos_err(rh, golden[f"c2/{alg}/r_hist"], half_width(wl))
+    err_v = rel_vel_err(vh, golden[f"c2/{alg}/v_hist"])
+    print(f"mixed {alg} electrons: pos {err_r:.3e} vel {err_v:.3e}")
+    assert err_r <= bound
+
+
+def test_mixed_rejects_unsupported(cuda):
+    wl = workloads.quad_solenoid_protons(n=8)
+    e, b = gpu_fields(wl)
+    with pytest.raises(NotImplementedError):
+        PusherGPU(wl.species, "yoshida", precision="mixed").track_batch(wl.r0, wl.v0, e, b, 2, wl.dt)

@@ -1,0 +1,116 @@
+"""Physics known-answer tests and invariances of the GPU path (the reference
+has no tests for its pushers; these are the analytic checks the path must
+satisfy): |v| or |u| conservation in a pure magnetic field, gyro-radius,
+E x B drift, trilinear exactness on linear fields, and bitwise invariance of
+each particle's result under chunking and cell re-sorting."""
+import numpy as np
+import pytest
+
+from pypatools_b200 import PusherGPU, Field, IonSpecies, workloads
+from pypatools_b200.constants import CLIGHT
+from tests.helpers import gpu_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _uniform_b(bz, half=10.0, nodes=5):
+    g = np.linspace(-half, half, nodes)
+    shape = (nodes,) * 3
+    return Field.from_arrays({"x": g, "y": g, "z": g},
+                             {"x": np.zeros(shape), "y": np.zeros(shape), "z": np.full(shape, bz)})
+
+
+def _beam(n, speed, seed=1):
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    return rng.uniform(-0.01, 0.01, (n, 3)), d * speed
+
+
+def test_boris_speed_conserved_in_pure_b(cuda):
+    ion = IonSpecies("proton")
+    r0, v0 = _beam(512, 1.0e7)
+    _, vh, _ = PusherGPU(ion, "boris").track_batch(r0, v0, Field.zero(3), _uniform_b(1.0), 5000, 1e-11, 5000)
+    s0 = np.linalg.norm(vh[0], axis=1)
+    s1 = np.linalg.norm(vh[-1], axis=1)
+    assert np.max(np.abs(s1 / s0 - 1.0)) < 5e-14
+
+
+@pytest.mark.parametrize("alg", ["boris_rel", "vay"])
+def test_u_conserved_in_pure_b_relativistic(cuda, alg):
+    ion = IonSpecies("electron")
+    r0, v0 = _beam(512, 0.998 * CLIGHT)
+    g0 = 1.0 / np.sqrt(1.0 - 0.998 ** 2)
+    _, vh, _ = PusherGPU(ion, alg).track_batch(r0, v0, Field.zero(3), _uniform_b(0.05), 10000, 1e-12, 10000)
+    # gamma from |v| of the snapshots; |u| = gamma |v| must stay put
+    v = np.linalg.norm(vh[-1], axis=1)
+    u = v / np.sqrt(1.0 - (v / CLIGHT) ** 2)
+    u0 = g0 * 0.998 * CLIGHT
+    assert np.max(np.abs(u / u0 - 1.0)) < 1e-9   # conversion v <-> u in the check costs ~gamma^2 eps
+
+
+def test_gyro_radius_uniform_b(cuda):
+    ion = IonSpecies("proton")
+    v_perp = 2.0e6
+    bz = 0.5
+    n_steps = 4000
+    r0 = np.zeros((1, 3))
+    v0 = np.array([[v_perp, 0.0, 0.0]])
+    rh, _, _ = PusherGPU(ion, "boris").track_batch(r0, v0, Field.zero(3), _uniform_b(bz), n_steps, 1e-11, 1)
+    radius = v_perp / (abs(ion.q_over_m) * bz)
+    xy = rh[:, 0, :2]
+    center = 0.5 * (xy.max(axis=0) + xy.min(axis=0))
+    rr = np.linalg.norm(xy - center, axis=1)
+    assert abs(rr.mean() / radius - 1.0) < 1e-4
+
+
+def test_e_cross_b_drift(cuda):
+    ion = IonSpecies("proton")
+    e0, b0 = 1.0e5, 1.0
+    e = Field(dim=0, field={"x": e0, "y": 0.0, "z": 0.0})
+    b = Field(dim=0, field={"x": 0.0, "y": 0.0, "z": b0})
+    period = 2 * np.pi / (ion.q_over_m * b0)
+    dt = period / 400
+    steps = 400 * 20
+    rh, _, _ = PusherGPU(ion, "boris").track_batch(np.zeros((1, 3)), np.zeros((1, 3)), e, b, steps, dt, 400)
+    drift = (rh[-1, 0] - rh[0, 0]) / (steps * dt)
+    # E x B / B^2 = (Ex x Bz)/B^2 = -Ex/Bz y-hat
+    assert abs(drift[1] / (-e0 / b0) - 1.0) < 1e-3
+    assert abs(drift[0]) < 1e-3 * e0 / b0
+
+
+def test_trilinear_exact_on_linear_field(cuda):
+    g = np.linspace(-1.0, 2.0, 7)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    f = Field.from_arrays({"x": g, "y": g, "z": g}, {"x": 1 + 2 * X - Y + 0.5 * Z, "y": X * 0 + 3.0, "z": -Z})
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(-1.0, 2.0, (1000, 3))
+    out = f(pts)
+    np.testing.assert_allclose(out[:, 0], 1 + 2 * pts[:, 0] - pts[:, 1] + 0.5 * pts[:, 2], rtol=1e-13, atol=1e-13)
+    np.testing.assert_allclose(out[:, 2], -pts[:, 2], rtol=1e-13, atol=1e-13)
+    outside = f(np.array([[2.5, 0.0, 0.0], [0.0, -1.0 - 1e-12, 0.0]]))
+    np.testing.assert_array_equal(outside, 0.0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chunking_and_sorting_are_bitwise_invariant(cuda, precision):
+    wl = workloads.quad_solenoid_protons(n=3000, nsteps=300)
+    e, b = gpu_fields(wl)
+    base = PusherGPU(wl.species, "boris", precision=precision).track_batch(wl.r0, wl.v0, e, b, 300, wl.dt, 50)
+    chunked = PusherGPU(wl.species, "boris", precision=precision, steps_per_launch=7).track_batch(
+        wl.r0, wl.v0, e, b, 300, wl.dt, 50)
+    sorted_ = PusherGPU(wl.species, "boris", precision=precision, sort_every=40).track_batch(
+        wl.r0, wl.v0, e, b, 300, wl.dt, 50)
+    for other in (chunked, sorted_):
+        np.testing.assert_array_equal(base[0], other[0])
+        np.testing.assert_array_equal(base[1], other[1])
+
+
+def test_nonfinite_input_warns(cuda):
+    wl = workloads.quad_solenoid_protons(n=4)
+    e, b = gpu_fields(wl)
+    r0 = wl.r0.copy()
+    r0[1, 0] = np.nan
+    with pytest.warns(RuntimeWarning, match="non-finite"):
+        rh, _, _ = PusherGPU(wl.species, "boris").track_batch(r0, wl.v0, e, b, 5, wl.dt)
+    assert np.isnan(rh[-1, 1, 0]) and np.isfinite(rh[-1, 0]).all()

@@ -1,0 +1,155 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports
+every symbol include/ppt.h declares, argument errors come back as status
+codes with messages, and the Python layer mirrors the reference's API."""
+import ctypes
+import re
+import warnings
+
+import numpy as np
+import pytest
+
+from pypatools_b200 import _lib
+from pypatools_b200.device_fields import decompose
+from pypatools_b200.field import Field, ScaledField, CompositeField, FieldMap, get_interpolator
+from pypatools_b200.pusher import PusherGPU, REFERENCE_ALGORITHMS
+from pypatools_b200.species import IonSpecies
+from tests.conftest import REPO
+
+
+def header_symbols():
+    text = (REPO / "include" / "ppt.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(ppt_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_header_symbol():
+    lib = _lib.load()
+    syms = header_symbols()
+    assert len(syms) >= 14
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) == set(_lib.SIGNATURES)
+    assert lib.ppt_abi_version() == 1
+
+
+def test_struct_layouts_match_header():
+    # natural C alignment of the ABI structs
+    assert ctypes.sizeof(_lib.GridDesc) == 48
+    assert ctypes.sizeof(_lib.Fields) == 4 * 8 + 8 + 48
+    assert ctypes.sizeof(_lib.State) == 40
+    assert ctypes.sizeof(_lib.TrackArgs) == 4 * 8 + 8 + 4 * 8 + 6 * 8
+
+
+def test_capi_argument_errors_without_gpu():
+    lib = _lib.load()
+    # non-increasing axis is rejected before any CUDA call
+    desc = _lib.GridDesc()
+    axes = [np.array([0.0, 1.0, 1.0]), np.array([0.0, 1.0]), np.array([0.0, 1.0])]
+    for d in range(3):
+        desc.n[d] = axes[d].shape[0]
+        desc.axis[d] = axes[d].ctypes.data
+    h = ctypes.c_void_p()
+    rc = lib.ppt_fieldmap_create(desc, 1, 0, _lib.DTYPE_F64, h)
+    assert rc == -1 and b"strictly increasing" in lib.ppt_last_error()
+    rc = lib.ppt_fieldmap_create(desc, 0, 0, _lib.DTYPE_F64, h)
+    assert rc == -1
+    assert lib.ppt_track(None, None, None, None) == -1
+    st = _lib.State(_lib.PREC_F64, 99, 10, None, None, None)
+    assert lib.ppt_track(st, _lib.Fields(), _lib.TrackArgs(), None) == -1
+    assert b"algorithm" in lib.ppt_last_error()
+    st = _lib.State(_lib.PREC_F64, 1, 0, None, None, None)
+    a = _lib.TrackArgs()
+    a.rec_every = 0
+    assert lib.ppt_track(st, _lib.Fields(), a, None) == -1
+    assert lib.ppt_moments(0, None, None, 1.0, None, None, None) == -1
+    assert lib.ppt_cell_sort_scratch_bytes(-1) == -1
+    assert lib.ppt_cell_sort_scratch_bytes(1000) > 1000 * 64
+    assert lib.ppt_moments_scratch_bytes(10) > 0
+    # empty state: nothing to do, no CUDA call
+    st = _lib.State(_lib.PREC_F64, 1, 0, None, None, None)
+    a.rec_every = 1
+    assert lib.ppt_track(st, _lib.Fields(), a, None) == 0
+
+
+def test_check_raises_with_message():
+    lib = _lib.load()
+    with pytest.raises(_lib.PptError, match="PPT_ERR_ARG"):
+        _lib.check(lib.ppt_moments(0, None, None, 1.0, None, None, None))
+
+
+class _FakeNumbaInterp:
+    """Looks like the reference's NumbaInterpolator to the adaptor."""
+
+    def __init__(self, grid, values):
+        self._grid = grid
+        self._values = values
+        self.fill_value = 0.0
+        self.method = "linear"
+
+
+class _FakeRefField:
+    def __init__(self, dim, field, scaling=1.0):
+        self._dim, self._field, self._scaling = dim, field, scaling
+
+
+def test_decompose_reference_duck_types():
+    g = (np.linspace(0, 1, 3),) * 3
+    v = np.arange(27.0).reshape(3, 3, 3)
+    f3 = _FakeRefField(3, {c: _FakeNumbaInterp(g, v) for c in "xyz"}, scaling=2.0)
+    t = decompose(f3)
+    assert len(t.terms) == 1 and t.terms[0].scale == 2.0 and not t.const.any()
+    f0 = _FakeRefField(0, {"x": 1.0, "y": 2.0, "z": 3.0}, scaling=0.5)
+    np.testing.assert_array_equal(decompose(f0).const, [0.5, 1.0, 1.5])
+
+    class _Scaled:
+        def __init__(self, field, scale, offset):
+            self.field, self.scale, self.offset = field, scale, offset
+
+    class _Comp:
+        def __init__(self, fields, weights):
+            self.fields, self.weights = fields, weights
+
+    s = decompose(_Scaled(f3, 3.0, 0.25))
+    assert s.terms[0].scale == 6.0
+    np.testing.assert_array_equal(s.const, [0.25] * 3)
+    c = decompose(_Comp([f3, f0], [0.5, -2.0]))
+    assert c.terms[0].scale == 1.0
+    np.testing.assert_array_equal(c.const, [-1.0, -2.0, -3.0])
+    with pytest.raises(NotImplementedError):
+        decompose(lambda pts: pts)
+
+
+def test_decompose_package_fields_and_zero():
+    g = {"x": np.linspace(0, 1, 4), "y": np.linspace(0, 1, 4), "z": np.linspace(0, 1, 5)}
+    vals = {c: np.ones((4, 4, 5)) for c in "xyz"}
+    f = Field.from_arrays(g, vals)
+    assert f.dim == 3 and len(decompose(f).terms) == 1
+    assert decompose(Field.zero(3)).terms == []
+    assert len(decompose(2.0 * f + f).terms) == 2
+    assert isinstance(f - f, CompositeField) and isinstance(f * 2.0, ScaledField)
+    fm = FieldMap(bfield=f)
+    assert decompose(fm.efield).terms == []
+    with pytest.raises(NotImplementedError):
+        get_interpolator((g["x"], g["y"], g["z"]), vals["x"], backend="numba")
+
+
+def test_pusher_constructor_mirrors_reference():
+    ion = IonSpecies("proton")
+    with pytest.raises(ValueError, match=r"Unknown algorithm 'nope'. Must be one of"):
+        PusherGPU(ion, "nope")
+    p = PusherGPU(ion, "RK4_REL")
+    assert p.algorithm == "rk4_rel" and p.relativistic
+    assert PusherGPU.ALGORITHMS == REFERENCE_ALGORITHMS
+
+    class _Hot:
+        name = "x"
+        q_over_m = 1.0
+        energy_mev = 1.0
+
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        assert PusherGPU(_Hot(), "leapfrog").algorithm == "vay_rel"
+        assert any("Leapfrog is non-relativistic" in str(x.message) for x in w)
+    with pytest.raises(NotImplementedError):
+        PusherGPU(ion, "boris", electrode_assembly=object())
+    p.change_algorithm("boris")
+    assert p.algorithm == "boris" and "PusherGPU(ion=proton" in repr(p)
