@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--sort-every", type=int, default=0)
+    ap.add_argument("--sort-every", type=int, default=500)
     return ap.parse_args()
 
 
@@ -108,12 +108,6 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline_sample(wl_fn, n_sample, steps, cores_hint):
-    """Time the CPU restatement of the reference algorithm on a bounded sample."""
-    from oracle import cpu_baseline
-    return cpu_baseline.run(wl_fn, n_sample, steps)
-
-
 def run_reference_arm(args, rank):
     if rank != 0:
         return
@@ -172,7 +166,7 @@ def main():
             tr.load(d_r0, d_v0)
             done = 0
             while done < wl.nsteps:
-                if args.sort_every and done and done % args.sort_every == 0:
+                if args.sort_every and done % args.sort_every == 0:
                     tr.sort()
                 k = min(chunk, wl.nsteps - done)
                 if time_launches:
@@ -264,7 +258,8 @@ def main():
     if not args.no_e2e:
         del trm, dfm
         torch.cuda.empty_cache()
-        pusher = PusherGPU(wl.species, "boris", precision="mixed", steps_per_launch=chunk)
+        pusher = PusherGPU(wl.species, "boris", precision="mixed", steps_per_launch=chunk,
+                           sort_every=args.sort_every)
         rf = RFModulation(wl.rf_frequency, wl.rf_phase)
         for _ in range(1):
             pusher.track_batch(wl.r0, wl.v0, efield, bfield, wl.nsteps, wl.dt, wl.rec_every, rf=rf)

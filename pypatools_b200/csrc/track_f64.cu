@@ -137,36 +137,44 @@ __device__ __forceinline__ V3 half_kick(V3 w, V3 E, V3 B, double dt, double qm) 
 
 struct Ctx {
     const FieldsDev* F;
-    double dt, qm, omega, phase;
+    double dt, qm, omega, phase, t0;
     unsigned hits;
+    int const_nz;
 };
 
+// Fields at r and field time t0 + g dt + toff; the time and the RF cosine are
+// only formed when E is non-zero.  Returns the number of maps containing r.
 template <bool RF>
-__device__ __forceinline__ void fields_at(Ctx& c, V3 r, double t, V3& E, V3& B) {
-    c.hits += eval_fields_f64(*c.F, r, E, B);
+__device__ __forceinline__ int fields_at(Ctx& c, V3 r, int64_t g, double toff, V3& E, V3& B) {
+    const int h = eval_fields_f64(*c.F, r, E, B);
+    c.hits += h;
     if (RF) {
-        if (E.x != 0.0 || E.y != 0.0 || E.z != 0.0) E = E * cos(c.omega * t + c.phase);
+        if (E.x != 0.0 || E.y != 0.0 || E.z != 0.0) {
+            const double t = c.t0 + (double)g * c.dt + toff;
+            E = E * cos(c.omega * t + c.phase);
+        }
     }
+    return h;
 }
 
 template <int ALG, bool RF>
-__device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, double t) {
+__device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, int64_t g) {
     const double dt = c.dt, qm = c.qm;
     if constexpr (ALG == PPT_ALG_RK4 || ALG == PPT_ALG_RK4_REL) {
         constexpr bool REL = ALG == PPT_ALG_RK4_REL;
         V3 E, B;
         const double h = 0.5 * dt;
-        fields_at<RF>(c, r, t, E, B);
+        fields_at<RF>(c, r, g, 0.0, E, B);
         V3 k1v = REL ? rk4_rel_deriv(w, E, B, qm) : lorentz(w, E, B, qm);
         V3 k1r = w;
         V3 r2 = r + h * k1r, v2 = w + h * k1v;
-        fields_at<RF>(c, r2, t + h, E, B);
+        fields_at<RF>(c, r2, g, h, E, B);
         V3 k2v = REL ? rk4_rel_deriv(v2, E, B, qm) : lorentz(v2, E, B, qm);
         V3 r3 = r + h * v2, v3_ = w + h * k2v;
-        fields_at<RF>(c, r3, t + h, E, B);
+        fields_at<RF>(c, r3, g, h, E, B);
         V3 k3v = REL ? rk4_rel_deriv(v3_, E, B, qm) : lorentz(v3_, E, B, qm);
         V3 r4 = r + dt * v3_, v4 = w + dt * k3v;
-        fields_at<RF>(c, r4, t + dt, E, B);
+        fields_at<RF>(c, r4, g, dt, E, B);
         V3 k4v = REL ? rk4_rel_deriv(v4, E, B, qm) : lorentz(v4, E, B, qm);
         const double s6 = dt / 6.0;
         r = r + s6 * (k1r + 2.0 * v2 + 2.0 * v3_ + v4);
@@ -175,7 +183,7 @@ __device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, double t) {
     } else if constexpr (ALG == PPT_ALG_YOSHIDA || ALG == PPT_ALG_YOSHIDA_REL) {
         constexpr bool REL = ALG == PPT_ALG_YOSHIDA_REL;
         V3 E, B;
-        fields_at<RF>(c, r, t, E, B);
+        fields_at<RF>(c, r, g, 0.0, E, B);
         const double cs[3] = {kYoC1, kYoC2, kYoC1};
         const double ds[3] = {kYoD1, kYoD2, kYoD1};
 #pragma unroll
@@ -187,18 +195,21 @@ __device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, double t) {
         if (REL) w = clamp_speed(w);
     } else {
         V3 E, B;
-        fields_at<RF>(c, r, t, E, B);
+        // With no map containing r and no constant field, E = B = 0 exactly and
+        // the leapfrog, Boris and relativistic Boris updates return w unchanged
+        // (every term they add is a signed zero), so they are skipped.
+        const bool any = fields_at<RF>(c, r, g, 0.0, E, B) != 0 || c.const_nz;
         if constexpr (ALG == PPT_ALG_LEAPFROG) {
-            w = w + lorentz(w, E, B, qm) * dt;
+            if (any) w = w + lorentz(w, E, B, qm) * dt;
             r = r + w * dt;
         } else if constexpr (ALG == PPT_ALG_BORIS) {
-            w = boris_v(w, E, B, dt, qm);
+            if (any) w = boris_v(w, E, B, dt, qm);
             r = r + w * dt;
         } else if constexpr (ALG == PPT_ALG_VAY_REL) {
             w = vay_rel_v(w, E, B, dt, qm);
             r = r + w * dt;
         } else if constexpr (ALG == PPT_ALG_BORIS_REL) {
-            w = boris_rel_u(w, E, B, dt, qm);
+            if (any) w = boris_rel_u(w, E, B, dt, qm);
             r = r + w_to_v<ALG>(w) * dt;
         } else {  // PPT_ALG_VAY
             w = vay_u(w, E, B, dt, qm);
@@ -232,7 +243,7 @@ __global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ 
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool live = s < P.n;
     unsigned steps_done = 0;
-    Ctx c{&P.F, P.dt, P.qm, P.omega, 0.0, 0u};
+    Ctx c{&P.F, P.dt, P.qm, P.omega, 0.0, P.t0, 0u, P.F.e_const_nz | P.F.b_const_nz};
     if (live) {
         const int64_t n = P.n;
         double* st = P.f64;
@@ -244,7 +255,7 @@ __global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ 
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (alg_staggered(ALG)) {
                 V3 E, B;
-                fields_at<RF>(c, r, P.t0 + (double)P.step0 * P.dt, E, B);
+                fields_at<RF>(c, r, P.step0, 0.0, E, B);
                 w = half_kick<ALG>(w, E, B, -0.5 * P.dt, P.qm);
             }
             if (P.r_hist) {
@@ -253,17 +264,19 @@ __global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ 
             }
         }
         // steps until the next record: record after global step g when (g+1) % rec == 0
-        int64_t g = P.step0;
-        int64_t until = P.rec_every - 1 - (g % P.rec_every);
-        for (int64_t k = 0; k < P.nsteps; ++k, ++g) {
-            step<ALG, RF>(c, r, w, P.t0 + (double)g * P.dt);
+        const int nsteps = (int)P.nsteps;
+        const int rec_every = P.rec_every > 0x7fffffff ? 0x7fffffff : (int)P.rec_every;
+        const int64_t until64 = P.rec_every - 1 - (P.step0 % P.rec_every);
+        int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
+        for (int k = 0; k < nsteps; ++k) {
+            step<ALG, RF>(c, r, w, P.step0 + k);
             if (until == 0) {
-                const int64_t rec = (g + 1) / P.rec_every;
+                const int64_t rec = (P.step0 + k + 1) / P.rec_every;
                 if (P.r_hist && rec < P.n_rec) {
                     write_row(P.r_hist, rec, n, row, r);
                     write_row(P.v_hist, rec, n, row, w_to_v<ALG>(w));
                 }
-                until = P.rec_every - 1;
+                until = rec_every - 1;
             } else {
                 --until;
             }
@@ -272,7 +285,7 @@ __global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ 
         if (P.flags & PPT_TRACK_FINAL) {
             if constexpr (alg_staggered(ALG)) {
                 V3 E, B;
-                fields_at<RF>(c, r, P.t0 + (double)P.nsteps_total * P.dt, E, B);
+                fields_at<RF>(c, r, P.nsteps_total, 0.0, E, B);
                 w = half_kick<ALG>(w, E, B, 0.5 * P.dt, P.qm);
                 if (P.v_hist) write_row(P.v_hist, P.n_rec - 1, n, row, w_to_v<ALG>(w));
             }

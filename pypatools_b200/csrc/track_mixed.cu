@@ -27,6 +27,31 @@ struct MixCtx {
     unsigned hits;
 };
 
+// 256-bit read-only load of one [E | B] node record (32-B aligned).
+__device__ __forceinline__ void ldg_f32x8(const float* p, float (&v)[8]) {
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]),
+                   "=f"(v[7])
+                 : "l"(p));
+}
+
+// One component from 8 corners (corner q = di*4 + dj*2 + dk), x first, then
+// y, then z (interpolators.py:127-135).
+template <typename Get>
+__device__ __forceinline__ float tri8(Get get, float tx, float ty, float tz) {
+    float c00 = lerp_f(get(0), get(4), tx), c01 = lerp_f(get(1), get(5), tx);
+    float c10 = lerp_f(get(2), get(6), tx), c11 = lerp_f(get(3), get(7), tx);
+    return lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
+}
+
+// In-domain test of a cell + offset position (the reference's bounds test).
+__device__ __forceinline__ bool mixed_inside(const TrackMixDev& P, const int cell[3], const float f[3]) {
+    int i;
+    float t;
+    return mixed_axis(cell[0], f[0], P.G.n[0], i, t) && mixed_axis(cell[1], f[1], P.G.n[1], i, t) &&
+           mixed_axis(cell[2], f[2], P.G.n[2], i, t);
+}
+
 // Trilinear E/B at (cell, offset) from the float32 map; returns false when
 // outside (fields = the constant parts only).
 __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3], F3& E,
@@ -41,46 +66,43 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     const MapDev& m = P.map;
     const float* base = static_cast<const float*>(m.data) + ((int64_t)i * m.sx + (int64_t)j * m.sy + k) * m.stride;
     const int64_t ox = m.sx * m.stride, oy = m.sy * m.stride, oz = m.stride;
+    if (m.stride == 8) {
+        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner
+        float q[8][8];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        if (h == 0 && !m.has_e) continue;
-        if (h == 1 && !m.has_b) continue;
-        const float* b = base + (h == 0 ? 0 : m.b_off);
+        for (int c = 0; c < 8; ++c) {
+            const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
+            ldg_f32x8(base + di * ox + dj * oy + dk * oz, q[c]);
+        }
+        E = E + f3(tri8([&](int c) { return q[c][0]; }, tx, ty, tz), tri8([&](int c) { return q[c][1]; }, tx, ty, tz),
+                   tri8([&](int c) { return q[c][2]; }, tx, ty, tz));
+        B = B + f3(tri8([&](int c) { return q[c][4]; }, tx, ty, tz), tri8([&](int c) { return q[c][5]; }, tx, ty, tz),
+                   tri8([&](int c) { return q[c][6]; }, tx, ty, tz));
+    } else {
+        // [F 0]: one 128-bit load per corner
         float4 q[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
             const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
-            q[c] = __ldg(reinterpret_cast<const float4*>(b + di * ox + dj * oy + dk * oz));
+            q[c] = __ldg(reinterpret_cast<const float4*>(base + di * ox + dj * oy + dk * oz));
         }
-        // x first, then y, then z (interpolators.py:127-135)
-        F3 o;
-        {
-            float c00 = lerp_f(q[0].x, q[4].x, tx), c01 = lerp_f(q[1].x, q[5].x, tx);
-            float c10 = lerp_f(q[2].x, q[6].x, tx), c11 = lerp_f(q[3].x, q[7].x, tx);
-            o.x = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
-        }
-        {
-            float c00 = lerp_f(q[0].y, q[4].y, tx), c01 = lerp_f(q[1].y, q[5].y, tx);
-            float c10 = lerp_f(q[2].y, q[6].y, tx), c11 = lerp_f(q[3].y, q[7].y, tx);
-            o.y = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
-        }
-        {
-            float c00 = lerp_f(q[0].z, q[4].z, tx), c01 = lerp_f(q[1].z, q[5].z, tx);
-            float c10 = lerp_f(q[2].z, q[6].z, tx), c11 = lerp_f(q[3].z, q[7].z, tx);
-            o.z = lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
-        }
-        if (h == 0) E = E + o; else B = B + o;
+        F3 o = f3(tri8([&](int c) { return q[c].x; }, tx, ty, tz), tri8([&](int c) { return q[c].y; }, tx, ty, tz),
+                  tri8([&](int c) { return q[c].z; }, tx, ty, tz));
+        if (m.has_e) E = E + o; else B = B + o;
     }
     return true;
 }
 
+// Fields at the step's field time t0 + g dt (+ toff for RK4 stages); the
+// float64 time and phase are formed only when E is non-zero.
 template <bool RF>
-__device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], double t, F3& E,
-                                             F3& B) {
+__device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], int64_t g,
+                                             double toff, F3& E, F3& B) {
     bool in = gather_mixed(*c.P, cell, f, E, B);
     c.hits += in;
     if (RF) {
         if (E.x != 0.0f || E.y != 0.0f || E.z != 0.0f) {
+            const double t = c.P->t0 + (double)g * c.P->dt + toff;
             double ph = c.P->omega * t + c.phase;
             double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
             float cf = cosf((float)red);
@@ -179,22 +201,62 @@ __device__ __forceinline__ void offset_point(const TrackMixDev& P, const int cel
     }
 }
 
+// Per-step position increment v dt / d in cell units as a float-float pair,
+// recomputed only when the velocity changes.
+__device__ __forceinline__ void increment(const TrackMixDev& P, const float vh[3], const float vl[3], float dh[3],
+                                          float dl[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float p = vh[a] * P.kh[a];
+        float e = fmaf(vh[a], P.kh[a], -p);
+        dh[a] = p;
+        dl[a] = fmaf(vh[a], P.kl[a], fmaf(vl[a], P.kh[a], e));
+    }
+}
+
+// Per-particle loop state of the Boris family: increment and in-map flag.
+struct Drift {
+    float dh[3];
+    float dl[3];
+    bool inside;
+};
+
 template <int ALG, bool RF>
-__device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float vh[3], float vl[3],
-                                           double t) {
+__device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float vh[3], float vl[3], Drift& d,
+                                           int64_t g) {
     const TrackMixDev& P = *c.P;
     F3 v = f3(vh[0], vh[1], vh[2]);
-    if constexpr (ALG == PPT_ALG_BORIS) {
-        F3 E, B;
-        if (fields_mixed<RF>(c, cell, f, t, E, B)) vel_add(vh, vl, boris_dv(v, E, B, P.hqdt));
-        advance(P, cell, f, vh, vl);
-    } else if constexpr (ALG == PPT_ALG_LEAPFROG) {
-        F3 E, B;
-        if (fields_mixed<RF>(c, cell, f, t, E, B)) vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
-        advance(P, cell, f, vh, vl);
+    if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
+        // Outside the map with no constant field both updates leave v exactly
+        // unchanged, so only the position moves: the drift path below.
+        if (d.inside || P.const_nz) {
+            F3 E, B;
+            if (fields_mixed<RF>(c, cell, f, g, 0.0, E, B)) {
+                vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
+                increment(P, vh, vl, d.dh, d.dl);
+            }
+        }
+        bool moved = false;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float x = f[a] + d.dh[a];
+            x = x + d.dl[a];
+            if (x <= 0.0f || x >= 1.0f) {   // crossed a cell face (or sits exactly on one)
+                float cc = floorf(x);
+                x -= cc;
+                cell[a] += (int)cc;
+                if (x >= 1.0f) {
+                    x -= 1.0f;
+                    cell[a] += 1;
+                }
+                moved = true;
+            }
+            f[a] = x;
+        }
+        if (moved || d.inside) d.inside = mixed_inside(P, cell, f);
     } else if constexpr (ALG == PPT_ALG_VAY_REL) {
         F3 E, B;
-        fields_mixed<RF>(c, cell, f, t, E, B);
+        fields_mixed<RF>(c, cell, f, g, 0.0, E, B);
         F3 vn = vay_rel_f(v, E, B, P.qm, P.dtf);
         // increment relative to the float32 head keeps the low part's bits
         vel_add(vh, vl, vn - v);
@@ -205,19 +267,19 @@ __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], f
         F3 E, B;
         int sc[3];
         float sf[3];
-        fields_mixed<RF>(c, cell, f, t, E, B);
+        fields_mixed<RF>(c, cell, f, g, 0.0, E, B);
         F3 k1 = REL ? rk4_rel_deriv_f(v, E, B, P.qm) : lorentz_f(v, E, B, P.qm);
         F3 v2 = v + h * k1;
         offset_point(P, cell, f, h * v, sc, sf);
-        fields_mixed<RF>(c, sc, sf, t + 0.5 * P.dt, E, B);
+        fields_mixed<RF>(c, sc, sf, g, 0.5 * P.dt, E, B);
         F3 k2 = REL ? rk4_rel_deriv_f(v2, E, B, P.qm) : lorentz_f(v2, E, B, P.qm);
         F3 v3_ = v + h * k2;
         offset_point(P, cell, f, h * v2, sc, sf);
-        fields_mixed<RF>(c, sc, sf, t + 0.5 * P.dt, E, B);
+        fields_mixed<RF>(c, sc, sf, g, 0.5 * P.dt, E, B);
         F3 k3 = REL ? rk4_rel_deriv_f(v3_, E, B, P.qm) : lorentz_f(v3_, E, B, P.qm);
         F3 v4 = v + dt * k3;
         offset_point(P, cell, f, dt * v3_, sc, sf);
-        fields_mixed<RF>(c, sc, sf, t + P.dt, E, B);
+        fields_mixed<RF>(c, sc, sf, g, P.dt, E, B);
         F3 k4 = REL ? rk4_rel_deriv_f(v4, E, B, P.qm) : lorentz_f(v4, E, B, P.qm);
         // r_new - r = dt v + dt^2/6 (k1 + k2 + k3); v_new - v = dt/6 (k1 + 2k2 + 2k3 + k4)
         const float s6 = dt * (1.0f / 6.0f);
@@ -276,19 +338,25 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
-                if (fields_mixed<RF>(c, cell, f, P.t0 + (double)P.step0 * P.dt, E, B))
-                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -P.hqdt));
+                if (fields_mixed<RF>(c, cell, f, P.step0, 0.0, E, B))
+                    // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
+                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt));
             }
             if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
         }
-        int64_t g = P.step0;
-        int64_t until = P.rec_every - 1 - (g % P.rec_every);
-        for (int64_t k = 0; k < P.nsteps; ++k, ++g) {
-            mixed_step<ALG, RF>(c, cell, f, vh, vl, P.t0 + (double)g * P.dt);
+        Drift d;
+        increment(P, vh, vl, d.dh, d.dl);
+        d.inside = mixed_inside(P, cell, f);
+        const int nsteps = (int)P.nsteps;
+        const int rec_every = P.rec_every > 0x7fffffff ? 0x7fffffff : (int)P.rec_every;
+        const int64_t until64 = P.rec_every - 1 - (P.step0 % P.rec_every);
+        int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
+        for (int k = 0; k < nsteps; ++k) {
+            mixed_step<ALG, RF>(c, cell, f, vh, vl, d, P.step0 + k);
             if (until == 0) {
-                const int64_t rec = (g + 1) / P.rec_every;
+                const int64_t rec = (P.step0 + k + 1) / P.rec_every;
                 if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, vh, vl, true);
-                until = P.rec_every - 1;
+                until = rec_every - 1;
             } else {
                 --until;
             }
@@ -297,8 +365,9 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         if (P.flags & PPT_TRACK_FINAL) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
-                if (fields_mixed<RF>(c, cell, f, P.t0 + (double)P.nsteps_total * P.dt, E, B))
-                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, P.hqdt));
+                if (fields_mixed<RF>(c, cell, f, P.nsteps_total, 0.0, E, B))
+                    // Boris push with time step +dt/2 (pusher.py:993-1007)
+                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt));
                 if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
             }
         }

@@ -185,7 +185,7 @@ class DeviceTracker:
         _lib.check(self.lib.ppt_cell_sort(self.state, self.dfields.fields, self.order.data_ptr(),
                                           self.rf_phase.data_ptr() if self.rf_phase is not None else None,
                                           self.sort_scratch.data_ptr(), self._stream(stream)))
-        self.launches += 1
+        self.launches += 5      # keys, tile scan, top scan, scan add, scatter
 
     def store(self, r, v, stream=None):
         """Write the current state as (n,3) float64 r, v in row order."""
@@ -315,36 +315,65 @@ class PusherGPU:
         rf_omega, rf_phase = 0.0, None
         if rf is not None:
             rf_omega = rf.omega
-            rf_phase = np.broadcast_to(np.asarray(rf.phase, dtype=np.float64), (m,))
-            rf_phase = torch.from_numpy(np.ascontiguousarray(rf_phase))
+            rf_phase = np.array(np.broadcast_to(np.asarray(rf.phase, dtype=np.float64), (m,)))
+            rf_phase = torch.from_numpy(rf_phase)
         tr = DeviceTracker(self.algorithm, self.q_over_m, df, m, nsteps, dt, rec, self.precision,
                            rf_omega=rf_omega, rf_phase=rf_phase, t0=t0, record=True, device=self.device)
         self.last_tracker = tr
         chunk = self.steps_per_launch or default_steps_per_launch(m, nsteps)
         if self.sort_every > 0:
             chunk = min(chunk, self.sort_every)
+        to_host = self.snapshot == "host"
         with torch.cuda.device(df.device):
+            if to_host:
+                # Snapshot rows stream to pinned host memory on a copy stream
+                # while later launches run; torch's pinned-block cache makes
+                # repeated calls of one size cheap.
+                h_r = torch.empty((n_rec, m, 3), dtype=torch.float64, pin_memory=True)
+                h_v = torch.empty((n_rec, m, 3), dtype=torch.float64, pin_memory=True)
+                copy_stream = torch.cuda.Stream(device=df.device)
+                compute = torch.cuda.current_stream()
+                copied = 0
+
+                def drain(upto):
+                    nonlocal copied
+                    if upto <= copied:
+                        return
+                    ev = torch.cuda.Event()
+                    ev.record(compute)
+                    copy_stream.wait_event(ev)
+                    with torch.cuda.stream(copy_stream):
+                        h_r[copied:upto].copy_(tr.r_hist[copied:upto], non_blocking=True)
+                        h_v[copied:upto].copy_(tr.v_hist[copied:upto], non_blocking=True)
+                    copied = upto
             tr.load(self._upload(r0, df.device), self._upload(v0, df.device))
             done = 0
             if nsteps == 0:
                 tr.advance(0)
             while done < nsteps:
-                if self.sort_every > 0 and done > 0 and done % self.sort_every == 0:
+                if self.sort_every > 0 and done % self.sort_every == 0:
                     tr.sort()
                 k = min(chunk, nsteps - done)
                 if verbose:
                     print(f"Step {done}/{nsteps} ({100 * done / nsteps:.0f}%)")
                 tr.advance(k)
                 done += k
+                if to_host and done < nsteps:
+                    # records 0 .. done // rec are final; the last one waits for
+                    # the closing half step of the Boris family
+                    drain(min(done // rec + 1, n_rec - 1))
+            if to_host:
+                drain(n_rec)
+                copy_stream.synchronize()
             status = tr.device_status()
         if status & _lib.STATUS_NONFINITE:
             warnings.warn("non-finite particle state encountered during tracking", RuntimeWarning)
         if verbose:
             print(f"Tracking complete: {nsteps} steps, {m} particles")
         active = np.ones(m, dtype=bool)
-        if self.snapshot == "device":
+        if not to_host:
             return tr.r_hist, tr.v_hist, active
-        return tr.r_hist.cpu().numpy(), tr.v_hist.cpu().numpy(), active
+        return h_r.numpy(), h_v.numpy(), active
 
     # -- single-particle API -------------------------------------------------
     def push(self, r, v, efield, bfield, dt):

@@ -53,10 +53,10 @@ def test_gyro_radius_uniform_b(cuda):
     ion = IonSpecies("proton")
     v_perp = 2.0e6
     bz = 0.5
-    n_steps = 4000
+    n_steps = 4000                     # period 1.31e-7 s = 1310 steps of 1e-10 s: three orbits
     r0 = np.zeros((1, 3))
     v0 = np.array([[v_perp, 0.0, 0.0]])
-    rh, _, _ = PusherGPU(ion, "boris").track_batch(r0, v0, Field.zero(3), _uniform_b(bz), n_steps, 1e-11, 1)
+    rh, _, _ = PusherGPU(ion, "boris").track_batch(r0, v0, Field.zero(3), _uniform_b(bz), n_steps, 1e-10, 1)
     radius = v_perp / (abs(ion.q_over_m) * bz)
     xy = rh[:, 0, :2]
     center = 0.5 * (xy.max(axis=0) + xy.min(axis=0))
