@@ -79,6 +79,8 @@ extern "C" {
 /* Device status bits (OR-ed into *status) */
 #define PPT_STATUS_NONFINITE  1  /* a particle's state became NaN/Inf */
 #define PPT_STATUS_BOUNDS     2  /* a debug-build bounds check failed */
+#define PPT_STATUS_RANGE      4  /* mixed form: a particle went 2^24 cells or more from the map
+                                    (beyond the exact range of its float cell index) */
 
 #define PPT_MAX_MAPS 4
 

@@ -19,7 +19,7 @@ ALG_IDS = {"leapfrog": 0, "boris": 1, "rk4": 2, "yoshida": 3, "vay_rel": 4, "rk4
 PREC_F64, PREC_MIXED = 0, 1
 DTYPE_F64, DTYPE_F32 = 0, 1
 TRACK_INIT, TRACK_FINAL = 1, 2
-STATUS_NONFINITE, STATUS_BOUNDS = 1, 2
+STATUS_NONFINITE, STATUS_BOUNDS, STATUS_RANGE = 1, 2, 4
 MAX_MAPS = 4
 MOMENTS_LEN = 22
 

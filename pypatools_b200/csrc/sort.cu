@@ -1,50 +1,58 @@
-// Particle reordering by cell, so that the threads of a warp gather corner
-// records from the same or neighbouring cells (L1/L2 sector reuse).
+// Particle reordering by cell, so that the threads of a warp gather the same
+// corner records (one L1 wavefront per corner load instead of one per
+// distinct cell).
 //
-// Counting sort on a spatial bucket key: the map-0 cell of each particle is
-// coarsened to 2x2x2-cell blocks, the block coordinates are Morton-interleaved
-// and shifted down to at most 2^20 buckets (octree nodes, so neighbouring
-// buckets stay spatially close); particles outside the map share one last
-// bucket.  Histogram (atomics) -> exclusive scan -> scatter into a scratch
-// copy -> copy back.  Order inside a bucket is arbitrary; `order` records
-// slot -> row so outputs are written in the caller's row order, and every
-// particle's arithmetic is independent of its slot.
+// Counting sort on the particle's map-0 cell: bucket = linear cell index
+// (k fastest) modulo 2^22 -- exact for maps up to 4M cells, a hash beyond;
+// particles outside the map share one last bucket.  Histogram -> exclusive
+// scan -> scatter into a scratch copy -> copy back, with warp-aggregated
+// atomics (lanes with equal keys combine before touching memory).  When
+// fewer than 1/16 of the particles are inside the map the reordering buys
+// nothing, and every kernel after the histogram returns at once: the sort is
+// a no-op decided on the device, so the caller's stream never waits.
+// Order inside a bucket is arbitrary; `order` records slot -> row so outputs
+// land in the caller's row order, and each particle's arithmetic is
+// independent of its slot.
 #include <cstring>
 
 #include "track_params.cuh"
 
 namespace ppt {
 
-constexpr int kMaxBucketBits = 20;
+constexpr int kBucketBits = 22;
 constexpr int kScanTile = 1024;
-
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
 
 struct SortGeom {
     double lo[3];
     double inv_d[3];
-    int n[3];          // nodes per axis
-    int shift;
-    uint32_t outside;  // bucket of particles outside the map
+    int n[3];           // nodes per axis
+    uint32_t n_in;      // buckets for in-map cells
+    uint32_t outside;   // bucket of particles outside the map (= n_in)
 };
 
+__device__ __forceinline__ bool cell_inside(const SortGeom& G, int c0, int c1, int c2) {
+    return (unsigned)c0 <= (unsigned)(G.n[0] - 2) && (unsigned)c1 <= (unsigned)(G.n[1] - 2) &&
+           (unsigned)c2 <= (unsigned)(G.n[2] - 2);
+}
+
 __device__ __forceinline__ uint32_t bucket_of_cells(const SortGeom& G, int c0, int c1, int c2) {
-    if ((unsigned)c0 > (unsigned)(G.n[0] - 2) || (unsigned)c1 > (unsigned)(G.n[1] - 2) ||
-        (unsigned)c2 > (unsigned)(G.n[2] - 2))
-        return G.outside;
-    uint32_t m = spread3((uint32_t)c0 >> 1) | (spread3((uint32_t)c1 >> 1) << 1) | (spread3((uint32_t)c2 >> 1) << 2);
-    return m >> G.shift;
+    if (!cell_inside(G, c0, c1, c2)) return G.outside;
+    const uint64_t lin = ((uint64_t)c0 * (uint64_t)(G.n[1] - 1) + (uint64_t)c1) * (uint64_t)(G.n[2] - 1) + (uint64_t)c2;
+    return (uint32_t)(lin % G.n_in);
+}
+
+// Histogram + in-map count with one atomic per distinct key per warp.
+__device__ __forceinline__ void count_key(uint32_t b, bool inside, uint32_t* count, uint32_t* ctrl) {
+    const unsigned active = __activemask();
+    const unsigned same = __match_any_sync(active, b);
+    const int lane = threadIdx.x & 31;
+    if (lane == __ffs(same) - 1) atomicAdd(count + b, (uint32_t)__popc(same));
+    const unsigned in_mask = __ballot_sync(active, inside);
+    if (lane == __ffs(active) - 1 && in_mask) atomicAdd(ctrl, (uint32_t)__popc(in_mask));
 }
 
 __global__ void sort_keys_f64(int64_t n, const double* __restrict__ st, SortGeom G, uint32_t* __restrict__ key,
-                              uint32_t* __restrict__ count) {
+                              uint32_t* __restrict__ count, uint32_t* __restrict__ ctrl) {
     int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= n) return;
     int c[3];
@@ -54,16 +62,20 @@ __global__ void sort_keys_f64(int64_t n, const double* __restrict__ st, SortGeom
     }
     uint32_t b = bucket_of_cells(G, c[0], c[1], c[2]);
     key[s] = b;
-    atomicAdd(count + b, 1u);
+    count_key(b, b != G.outside, count, ctrl);
 }
 
 __global__ void sort_keys_mixed(int64_t n, const int32_t* __restrict__ ci, SortGeom G, uint32_t* __restrict__ key,
-                                uint32_t* __restrict__ count) {
+                                uint32_t* __restrict__ count, uint32_t* __restrict__ ctrl) {
     int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= n) return;
     uint32_t b = bucket_of_cells(G, ci[s], ci[n + s], ci[2 * n + s]);
     key[s] = b;
-    atomicAdd(count + b, 1u);
+    count_key(b, b != G.outside, count, ctrl);
+}
+
+__device__ __forceinline__ bool sort_wanted(const uint32_t* ctrl, int64_t n) {
+    return (int64_t)ctrl[0] * 16 >= n;
 }
 
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
@@ -92,7 +104,9 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
 }
 
 __global__ void __launch_bounds__(kScanTile) scan_tiles(int64_t nb, const uint32_t* __restrict__ count,
-                                                        uint32_t* __restrict__ offset, uint32_t* __restrict__ tile_sum) {
+                                                        uint32_t* __restrict__ offset, uint32_t* __restrict__ tile_sum,
+                                                        const uint32_t* __restrict__ ctrl, int64_t n) {
+    if (!sort_wanted(ctrl, n)) return;
     __shared__ uint32_t sh[32];
     int64_t i = blockIdx.x * (int64_t)kScanTile + threadIdx.x;
     uint32_t v = i < nb ? count[i] : 0u;
@@ -102,8 +116,10 @@ __global__ void __launch_bounds__(kScanTile) scan_tiles(int64_t nb, const uint32
     if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
 }
 
-// exclusive scan of up to kScanTile * 2 tile sums in one block
-__global__ void __launch_bounds__(kScanTile) scan_top(int ntiles, uint32_t* __restrict__ tile_sum) {
+// exclusive scan of the tile sums in one block
+__global__ void __launch_bounds__(kScanTile) scan_top(int ntiles, uint32_t* __restrict__ tile_sum,
+                                                      const uint32_t* __restrict__ ctrl, int64_t n) {
+    if (!sort_wanted(ctrl, n)) return;
     __shared__ uint32_t sh[32];
     uint32_t carry = 0;
     for (int base = 0; base < ntiles; base += kScanTile) {
@@ -116,7 +132,9 @@ __global__ void __launch_bounds__(kScanTile) scan_top(int ntiles, uint32_t* __re
     }
 }
 
-__global__ void scan_add(int64_t nb, uint32_t* __restrict__ offset, const uint32_t* __restrict__ tile_sum) {
+__global__ void scan_add(int64_t nb, uint32_t* __restrict__ offset, const uint32_t* __restrict__ tile_sum,
+                         const uint32_t* __restrict__ ctrl, int64_t n) {
+    if (!sort_wanted(ctrl, n)) return;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < nb) offset[i] += tile_sum[i / kScanTile];
 }
@@ -125,14 +143,23 @@ __global__ void scan_add(int64_t nb, uint32_t* __restrict__ offset, const uint32
 // na + nb columns of 4-byte words taken from two sources (mixed state: the
 // int32 cells, then the float32 columns) into one destination block.
 __global__ void sort_scatter(int64_t n, const uint32_t* __restrict__ key, uint32_t* __restrict__ offset,
-                             int ncols64, const double* __restrict__ src64, double* __restrict__ dst64, int na,
-                             const uint32_t* __restrict__ src_a, int nb, const uint32_t* __restrict__ src_b,
-                             uint32_t* __restrict__ dst32, const int64_t* __restrict__ order,
-                             int64_t* __restrict__ order_out, const double* __restrict__ phase,
-                             double* __restrict__ phase_out) {
+                             const uint32_t* __restrict__ ctrl, int ncols64, const double* __restrict__ src64,
+                             double* __restrict__ dst64, int na, const uint32_t* __restrict__ src_a, int nb,
+                             const uint32_t* __restrict__ src_b, uint32_t* __restrict__ dst32,
+                             const int64_t* __restrict__ order, int64_t* __restrict__ order_out,
+                             const double* __restrict__ phase, double* __restrict__ phase_out) {
+    if (!sort_wanted(ctrl, n)) return;
     int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const int64_t d = atomicAdd(offset + key[s], 1u);
+    const uint32_t b = key[s];
+    const unsigned active = __activemask();
+    const unsigned same = __match_any_sync(active, b);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(same) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(offset + b, (uint32_t)__popc(same));
+    base = __shfl_sync(same, base, leader);
+    const int64_t d = (int64_t)base + __popc(same & ((1u << lane) - 1u));
     for (int c = 0; c < ncols64; ++c) dst64[c * n + d] = src64[c * n + s];
     for (int c = 0; c < na; ++c) dst32[c * n + d] = src_a[c * n + s];
     for (int c = 0; c < nb; ++c) dst32[(na + c) * n + d] = src_b[c * n + s];
@@ -140,25 +167,43 @@ __global__ void sort_scatter(int64_t n, const uint32_t* __restrict__ key, uint32
     if (phase) phase_out[d] = phase[s];
 }
 
+// Copy the permuted block back (only when the sort ran).
+__global__ void sort_copy_back(int64_t words, const uint32_t* __restrict__ src, uint32_t* __restrict__ dst,
+                               const uint32_t* __restrict__ ctrl, int64_t n) {
+    if (!sort_wanted(ctrl, n)) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SortLayout {
-    size_t key, count, tiles, tmp64, tmp32, order, phase, total;
+    size_t key, count, tiles, ctrl, tmp64, tmp32, order, phase, total;
 };
 
 static SortLayout sort_layout(int64_t n) {
     SortLayout L;
-    const size_t nb = ((size_t)1 << kMaxBucketBits) + 1;
+    const size_t nb = ((size_t)1 << kBucketBits) + 1;
     size_t o = 0;
     L.key = o;   o += align256((size_t)n * 4);
     L.count = o; o += align256(nb * 4);
     L.tiles = o; o += align256((nb / kScanTile + 2) * 4);
-    L.tmp64 = o; o += align256((size_t)n * 6 * 8);     // float64 state, or mixed f32 part (9 words) below
+    L.ctrl = o;  o += 256;
+    L.tmp64 = o; o += align256((size_t)n * 6 * 8);     // float64 state
     L.tmp32 = o; o += align256((size_t)n * 12 * 4);    // mixed: 3 int32 + 9 float32 columns
     L.order = o; o += align256((size_t)n * 8);
     L.phase = o; o += align256((size_t)n * 8);
     L.total = o;
     return L;
+}
+
+static void copy_back(const void* src, void* dst, size_t bytes, const uint32_t* ctrl, int64_t n, cudaStream_t s) {
+    const int64_t words = (int64_t)(bytes / 4);
+    const int block = 256;
+    int64_t g = (words + block - 1) / block;
+    const int grid = (int)(g > 148 * 16 ? 148 * 16 : (g < 1 ? 1 : g));
+    sort_copy_back<<<grid, block, 0, s>>>(words, static_cast<const uint32_t*>(src), static_cast<uint32_t*>(dst), ctrl,
+                                          n);
 }
 
 }  // namespace ppt
@@ -182,26 +227,18 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
     if (rc) return rc;
     if (F.n_maps == 0) return PPT_OK;   // no map: nothing to be local to
     const MapDev& m = F.maps[0];
+    if (!m.all_uniform) return PPT_OK;  // non-uniform maps: no cheap cell key, keep the order
     SortGeom G;
-    int bits = 0;
+    uint64_t cells = 1;
     for (int a = 0; a < 3; ++a) {
         G.lo[a] = m.ax[a].lo;
         G.inv_d[a] = m.ax[a].inv_d;
         G.n[a] = m.ax[a].n;
-        int coarse = (m.ax[a].n - 1 + 1) / 2;
-        int b = 0;
-        while ((1 << b) < coarse) ++b;
-        bits = b > bits ? b : bits;
+        cells *= (uint64_t)(m.ax[a].n - 1);
     }
-    if (bits > 10) return fail(PPT_ERR_UNSUPPORTED, "cell sort handles maps up to 2048 nodes per axis");
-    const int key_bits = 3 * bits;
-    G.shift = key_bits > kMaxBucketBits ? key_bits - kMaxBucketBits : 0;
-    G.outside = (uint32_t)((1u << (key_bits - G.shift)));
-    const int64_t nb = (int64_t)G.outside + 1;
-    if (st->precision == PPT_PREC_MIXED && !m.all_uniform)
-        return fail(PPT_ERR_UNSUPPORTED, "mixed state needs a uniform map");
-    if (st->precision == PPT_PREC_F64 && !m.all_uniform)
-        return fail(PPT_ERR_UNSUPPORTED, "cell sort needs uniform axes (non-uniform maps: skip sorting)");
+    G.n_in = (uint32_t)(cells < ((uint64_t)1 << kBucketBits) ? cells : ((uint64_t)1 << kBucketBits));
+    G.outside = G.n_in;
+    const int64_t nb = (int64_t)G.n_in + 1;
 
     const int64_t n = st->n;
     SortLayout L = sort_layout(n);
@@ -209,6 +246,7 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
     uint32_t* key = reinterpret_cast<uint32_t*>(base + L.key);
     uint32_t* count = reinterpret_cast<uint32_t*>(base + L.count);
     uint32_t* tiles = reinterpret_cast<uint32_t*>(base + L.tiles);
+    uint32_t* ctrl = reinterpret_cast<uint32_t*>(base + L.ctrl);
     double* tmp64 = reinterpret_cast<double*>(base + L.tmp64);
     uint32_t* tmp32 = reinterpret_cast<uint32_t*>(base + L.tmp32);
     int64_t* order_tmp = reinterpret_cast<int64_t*>(base + L.order);
@@ -217,30 +255,29 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
     const int block = 256;
 
     PPT_CUDA_TRY(cudaMemsetAsync(count, 0, (size_t)nb * 4, s));
+    PPT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, 4, s));
     if (st->precision == PPT_PREC_F64)
-        sort_keys_f64<<<grid_for(n, block), block, 0, s>>>(n, st->f64, G, key, count);
+        sort_keys_f64<<<grid_for(n, block), block, 0, s>>>(n, st->f64, G, key, count, ctrl);
     else
-        sort_keys_mixed<<<grid_for(n, block), block, 0, s>>>(n, st->i32, G, key, count);
+        sort_keys_mixed<<<grid_for(n, block), block, 0, s>>>(n, st->i32, G, key, count, ctrl);
     const int ntiles = (int)((nb + kScanTile - 1) / kScanTile);
-    scan_tiles<<<ntiles, kScanTile, 0, s>>>(nb, count, count, tiles);
-    scan_top<<<1, kScanTile, 0, s>>>(ntiles, tiles);
-    scan_add<<<grid_for(nb, block), block, 0, s>>>(nb, count, tiles);
+    scan_tiles<<<ntiles, kScanTile, 0, s>>>(nb, count, count, tiles, ctrl, n);
+    scan_top<<<1, kScanTile, 0, s>>>(ntiles, tiles, ctrl, n);
+    scan_add<<<grid_for(nb, block), block, 0, s>>>(nb, count, tiles, ctrl, n);
     if (st->precision == PPT_PREC_F64) {
-        sort_scatter<<<grid_for(n, block), block, 0, s>>>(n, key, count, 6, st->f64, tmp64, 0, nullptr, 0, nullptr,
-                                                          nullptr, order, order_tmp, rf_phase, phase_tmp);
-        PPT_CUDA_TRY(cudaGetLastError());
-        PPT_CUDA_TRY(cudaMemcpyAsync(st->f64, tmp64, (size_t)n * 6 * 8, cudaMemcpyDeviceToDevice, s));
+        sort_scatter<<<grid_for(n, block), block, 0, s>>>(n, key, count, ctrl, 6, st->f64, tmp64, 0, nullptr, 0,
+                                                          nullptr, nullptr, order, order_tmp, rf_phase, phase_tmp);
+        copy_back(tmp64, st->f64, (size_t)n * 6 * 8, ctrl, n, s);
     } else {
         // 3 int32 cell columns then 9 float32 columns, all 4-byte words
         sort_scatter<<<grid_for(n, block), block, 0, s>>>(
-            n, key, count, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 9,
+            n, key, count, ctrl, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 9,
             reinterpret_cast<const uint32_t*>(st->f32), tmp32, order, order_tmp, rf_phase, phase_tmp);
-        PPT_CUDA_TRY(cudaGetLastError());
-        PPT_CUDA_TRY(cudaMemcpyAsync(st->i32, tmp32, (size_t)n * 3 * 4, cudaMemcpyDeviceToDevice, s));
-        PPT_CUDA_TRY(cudaMemcpyAsync(st->f32, tmp32 + 3 * n, (size_t)n * 9 * 4, cudaMemcpyDeviceToDevice, s));
+        copy_back(tmp32, st->i32, (size_t)n * 3 * 4, ctrl, n, s);
+        copy_back(tmp32 + 3 * n, st->f32, (size_t)n * 9 * 4, ctrl, n, s);
     }
+    copy_back(order_tmp, order, (size_t)n * 8, ctrl, n, s);
+    if (rf_phase) copy_back(phase_tmp, rf_phase, (size_t)n * 8, ctrl, n, s);
     PPT_CUDA_TRY(cudaGetLastError());
-    PPT_CUDA_TRY(cudaMemcpyAsync(order, order_tmp, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
-    if (rf_phase) PPT_CUDA_TRY(cudaMemcpyAsync(rf_phase, phase_tmp, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
     return PPT_OK;
 }

@@ -221,40 +221,46 @@ struct Drift {
     bool inside;
 };
 
+constexpr float kBelowOne = 0.99999994f;   // largest float below 1
+
+// One step of the Boris family (Boris, leapfrog) with float-valued cell
+// indices (exact integers below 2^24).  Outside the map with no constant
+// field both updates leave v exactly unchanged (every added term is zero), so
+// such a step is only the position advance: two adds of the float-float
+// increment and a branch-free carry of whole cells.
+template <int ALG, bool RF>
+__device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
+                                            int64_t g) {
+    const TrackMixDev& P = *c.P;
+    // cheap pre-test on the cell range (the last node layer included); the
+    // exact bounds rule is applied inside gather_mixed
+    const bool maybe = (cf[0] >= 0.0f) & (cf[0] <= P.cell_max[0]) & (cf[1] >= 0.0f) & (cf[1] <= P.cell_max[1]) &
+                       (cf[2] >= 0.0f) & (cf[2] <= P.cell_max[2]);
+    if (maybe || P.const_nz) {
+        const int cell[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
+        F3 E, B;
+        if (fields_mixed<RF>(c, cell, f, g, 0.0, E, B)) {
+            F3 v = f3(vh[0], vh[1], vh[2]);
+            vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
+            increment(P, vh, vl, d.dh, d.dl);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float x = f[a] + d.dh[a];
+        x = x + d.dl[a];
+        const float cc = floorf(x);
+        f[a] = fminf(x - cc, kBelowOne);   // x - floor(x) rounds to 1 only for x just below an integer
+        cf[a] += cc;
+    }
+}
+
 template <int ALG, bool RF>
 __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float vh[3], float vl[3], Drift& d,
                                            int64_t g) {
     const TrackMixDev& P = *c.P;
     F3 v = f3(vh[0], vh[1], vh[2]);
-    if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
-        // Outside the map with no constant field both updates leave v exactly
-        // unchanged, so only the position moves: the drift path below.
-        if (d.inside || P.const_nz) {
-            F3 E, B;
-            if (fields_mixed<RF>(c, cell, f, g, 0.0, E, B)) {
-                vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
-                increment(P, vh, vl, d.dh, d.dl);
-            }
-        }
-        bool moved = false;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float x = f[a] + d.dh[a];
-            x = x + d.dl[a];
-            if (x <= 0.0f || x >= 1.0f) {   // crossed a cell face (or sits exactly on one)
-                float cc = floorf(x);
-                x -= cc;
-                cell[a] += (int)cc;
-                if (x >= 1.0f) {
-                    x -= 1.0f;
-                    cell[a] += 1;
-                }
-                moved = true;
-            }
-            f[a] = x;
-        }
-        if (moved || d.inside) d.inside = mixed_inside(P, cell, f);
-    } else if constexpr (ALG == PPT_ALG_VAY_REL) {
+    if constexpr (ALG == PPT_ALG_VAY_REL) {
         F3 E, B;
         fields_mixed<RF>(c, cell, f, g, 0.0, E, B);
         F3 vn = vay_rel_f(v, E, B, P.qm, P.dtf);
@@ -351,14 +357,31 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         const int rec_every = P.rec_every > 0x7fffffff ? 0x7fffffff : (int)P.rec_every;
         const int64_t until64 = P.rec_every - 1 - (P.step0 % P.rec_every);
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
-        for (int k = 0; k < nsteps; ++k) {
-            mixed_step<ALG, RF>(c, cell, f, vh, vl, d, P.step0 + k);
-            if (until == 0) {
-                const int64_t rec = (P.step0 + k + 1) / P.rec_every;
-                if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, vh, vl, true);
-                until = rec_every - 1;
-            } else {
-                --until;
+        if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
+            float cf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
+            for (int k = 0; k < nsteps; ++k) {
+                family_step<ALG, RF>(c, cf, f, vh, vl, d, P.step0 + k);
+                if (until == 0) {
+                    const int64_t rec = (P.step0 + k + 1) / P.rec_every;
+                    const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
+                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
+                    until = rec_every - 1;
+                } else {
+                    --until;
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) cell[a] = (int)cf[a];
+        } else {
+            for (int k = 0; k < nsteps; ++k) {
+                mixed_step<ALG, RF>(c, cell, f, vh, vl, d, P.step0 + k);
+                if (until == 0) {
+                    const int64_t rec = (P.step0 + k + 1) / P.rec_every;
+                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, vh, vl, true);
+                    until = rec_every - 1;
+                } else {
+                    --until;
+                }
             }
         }
         steps_done = (unsigned)P.nsteps;
@@ -381,6 +404,8 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         if (P.status) {
             float sum = f[0] + f[1] + f[2] + vh[0] + vh[1] + vh[2];
             if (!isfinite(sum)) atomicOr(P.status, PPT_STATUS_NONFINITE);
+            const int lim = 1 << 24;
+            if (abs(cell[0]) >= lim || abs(cell[1]) >= lim || abs(cell[2]) >= lim) atomicOr(P.status, PPT_STATUS_RANGE);
         }
     }
     if (P.counters) {
@@ -435,6 +460,7 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
         P->kh[c] = (float)k;
         P->kl[c] = (float)(k - (double)P->kh[c]);
         P->inv_d[c] = (float)P->G.inv_d[c];
+        P->cell_max[c] = (float)(P->G.n[c] - 1);
     }
     P->const_nz = F.e_const_nz || F.b_const_nz;
     P->n = st->n;

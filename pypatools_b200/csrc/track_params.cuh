@@ -50,6 +50,7 @@ struct TrackMixDev {
     float kh[3];     // dt / d: cell units per (m/s), as a float-float pair
     float kl[3];
     float inv_d[3];  // 1 / d (RK4 stage positions)
+    float cell_max[3];  // n - 1 per axis: last node layer, for the cheap in-map pre-test
     const double* rf_phase;
     int32_t* ci;
     float* fs;

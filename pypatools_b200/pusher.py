@@ -185,7 +185,9 @@ class DeviceTracker:
         _lib.check(self.lib.ppt_cell_sort(self.state, self.dfields.fields, self.order.data_ptr(),
                                           self.rf_phase.data_ptr() if self.rf_phase is not None else None,
                                           self.sort_scratch.data_ptr(), self._stream(stream)))
-        self.launches += 5      # keys, tile scan, top scan, scan add, scatter
+        # keys, tile scan, top scan, scan add, scatter, then one copy-back per
+        # permuted array (state block(s), order, RF phase)
+        self.launches += 5 + (1 if self.precision == "fp64" else 2) + 1 + (1 if self.rf_phase is not None else 0)
 
     def store(self, r, v, stream=None):
         """Write the current state as (n,3) float64 r, v in row order."""
@@ -368,6 +370,9 @@ class PusherGPU:
             status = tr.device_status()
         if status & _lib.STATUS_NONFINITE:
             warnings.warn("non-finite particle state encountered during tracking", RuntimeWarning)
+        if status & _lib.STATUS_RANGE:
+            warnings.warn("mixed form: a particle went 2^24 cells or more from the map; its position is no "
+                          "longer exact (use precision='fp64' for such tracks)", RuntimeWarning)
         if verbose:
             print(f"Tracking complete: {nsteps} steps, {m} particles")
         active = np.ones(m, dtype=bool)

@@ -79,8 +79,8 @@ def _per_particle(r, r_ref, half):
 # step apart, and the 1 MV/m field at the map face (fill 0 outside) turns that
 # into a 1e-3-level velocity difference.  The bounds below are on the median
 # and on the first record (before any exit); max and p90 are reported.
-@pytest.mark.parametrize("alg,p50_bound,first_bound", [("boris", 1e-5, 1e-5), ("vay_rel", 5e-2, 5e-2),
-                                                       ("rk4_rel", 1e-5, 1e-5)])
+@pytest.mark.parametrize("alg,p50_bound,first_bound", [("boris", 1e-5, 1e-4), ("vay_rel", 1e-2, 5e-2),
+                                                       ("rk4_rel", 5e-6, 5e-5)])
 def test_mixed_electron_sweep_error_report(cuda, golden, alg, p50_bound, first_bound):
     wl = workloads.radial_e_solenoid_electrons(n=128)
     e, b = gpu_fields(wl)
