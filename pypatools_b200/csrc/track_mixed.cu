@@ -64,31 +64,58 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     if (!mixed_axis(cell[1], f[1], P.G.n[1], j, ty)) return false;
     if (!mixed_axis(cell[2], f[2], P.G.n[2], k, tz)) return false;
     const MapDev& m = P.map;
-    const float* base = static_cast<const float*>(m.data) + ((int64_t)i * m.sx + (int64_t)j * m.sy + k) * m.stride;
-    const int64_t ox = m.sx * m.stride, oy = m.sy * m.stride, oz = m.stride;
+    // Trilinear weights of the 8 corners (corner q = di*4 + dj*2 + dk); each
+    // component is then one product and seven FMAs.
+    const float ux = 1.0f - tx, uy = 1.0f - ty, uz = 1.0f - tz;
+    const float a00 = ux * uy, a01 = ux * ty, a10 = tx * uy, a11 = tx * ty;
+    const float w[8] = {a00 * uz, a00 * tz, a01 * uz, a01 * tz, a10 * uz, a10 * tz, a11 * uz, a11 * tz};
+    const int64_t node = (int64_t)i * m.sx + (int64_t)j * m.sy + k;
     if (m.stride == 8) {
-        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner
+        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner; the k+1
+        // corner is the next record (immediate offset)
+        const float* p00 = static_cast<const float*>(m.data) + node * 8;
+        const float* p10 = p00 + m.sx * 8;
+        const float* p01 = p00 + m.sy * 8;
+        const float* p11 = p10 + m.sy * 8;
+        const float* pc[4] = {p00, p01, p10, p11};   // (di, dj) = (0,0) (0,1) (1,0) (1,1)
         float q[8][8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
-            ldg_f32x8(base + di * ox + dj * oy + dk * oz, q[c]);
+        for (int c = 0; c < 4; ++c) {
+            ldg_f32x8(pc[c], q[2 * c]);
+            ldg_f32x8(pc[c] + 8, q[2 * c + 1]);
         }
-        E = E + f3(tri8([&](int c) { return q[c][0]; }, tx, ty, tz), tri8([&](int c) { return q[c][1]; }, tx, ty, tz),
-                   tri8([&](int c) { return q[c][2]; }, tx, ty, tz));
-        B = B + f3(tri8([&](int c) { return q[c][4]; }, tx, ty, tz), tri8([&](int c) { return q[c][5]; }, tx, ty, tz),
-                   tri8([&](int c) { return q[c][6]; }, tx, ty, tz));
+        float acc[6];
+#pragma unroll
+        for (int comp = 0; comp < 6; ++comp) {
+            const int slot = comp < 3 ? comp : comp + 1;
+            float s = w[0] * q[0][slot];
+#pragma unroll
+            for (int c = 1; c < 8; ++c) s = fmaf(w[c], q[c][slot], s);
+            acc[comp] = s;
+        }
+        E = E + f3(acc[0], acc[1], acc[2]);
+        B = B + f3(acc[3], acc[4], acc[5]);
     } else {
         // [F 0]: one 128-bit load per corner
+        const float* p00 = static_cast<const float*>(m.data) + node * 4;
+        const float* p10 = p00 + m.sx * 4;
+        const float* p01 = p00 + m.sy * 4;
+        const float* p11 = p10 + m.sy * 4;
+        const float* pc[4] = {p00, p01, p10, p11};
         float4 q[8];
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
-            q[c] = __ldg(reinterpret_cast<const float4*>(base + di * ox + dj * oy + dk * oz));
+        for (int c = 0; c < 4; ++c) {
+            q[2 * c] = __ldg(reinterpret_cast<const float4*>(pc[c]));
+            q[2 * c + 1] = __ldg(reinterpret_cast<const float4*>(pc[c] + 4));
         }
-        F3 o = f3(tri8([&](int c) { return q[c].x; }, tx, ty, tz), tri8([&](int c) { return q[c].y; }, tx, ty, tz),
-                  tri8([&](int c) { return q[c].z; }, tx, ty, tz));
-        if (m.has_e) E = E + o; else B = B + o;
+        float ox = w[0] * q[0].x, oy = w[0] * q[0].y, oz = w[0] * q[0].z;
+#pragma unroll
+        for (int c = 1; c < 8; ++c) {
+            ox = fmaf(w[c], q[c].x, ox);
+            oy = fmaf(w[c], q[c].y, oy);
+            oz = fmaf(w[c], q[c].z, oz);
+        }
+        if (m.has_e) E = E + f3(ox, oy, oz); else B = B + f3(ox, oy, oz);
     }
     return true;
 }
@@ -102,8 +129,9 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
     c.hits += in;
     if (RF) {
         if (E.x != 0.0f || E.y != 0.0f || E.z != 0.0f) {
-            const double t = c.P->t0 + (double)g * c.P->dt + toff;
-            double ph = c.P->omega * t + c.phase;
+            // omega (t0 + g dt + toff) + phi_i = (omega t0 + phi_i) + g (omega dt) + omega toff, in float64
+            double ph = fma((double)g, c.P->wdt, c.phase);
+            if (toff != 0.0) ph = fma(c.P->omega, toff, ph);
             double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
             float cf = cosf((float)red);
             E = cf * E;
@@ -229,8 +257,8 @@ constexpr float kBelowOne = 0.99999994f;   // largest float below 1
 // such a step is only the position advance: two adds of the float-float
 // increment and a branch-free carry of whole cells.
 template <int ALG, bool RF>
-__device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
-                                            int64_t g) {
+__device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], float fl[3], float vh[3], float vl[3],
+                                            Drift& d, int64_t g) {
     const TrackMixDev& P = *c.P;
     // cheap pre-test on the cell range (the last node layer included); the
     // exact bounds rule is applied inside gather_mixed
@@ -244,6 +272,26 @@ __device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], 
             vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
             increment(P, vh, vl, d.dh, d.dl);
         }
+        // Where fields act, the offset carries its rounding error in fl
+        // (float-float accumulation), so the in-map position does not random-
+        // walk at float32 resolution; that keeps map-exit steps in step with
+        // the float64 form.
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float s = f[a] + d.dh[a];
+            const float bb = s - f[a];
+            float lo = fl[a] + (((f[a] - (s - bb)) + (d.dh[a] - bb)) + d.dl[a]);
+            const float cc = floorf(s);
+            const float sn = s - cc;
+            if (cc < 0.0f) {   // s + |cc| may round: keep that error too (two-sum)
+                const float b2 = sn - s;
+                lo += (s - (sn - b2)) + (-cc - b2);
+            }
+            f[a] = sn;
+            fl[a] = lo;
+            cf[a] += cc;
+        }
+        return;
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -311,13 +359,18 @@ __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], f
     }
 }
 
+// Snapshot row: x = lo + (cell + f + fl) d and v = vh + vl, formed in
+// float64 (output formatting only; fl may be NULL).
 __device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t rec, int64_t row, const int cell[3],
                                                 const float f[3], const float vh[3], const float vl[3],
-                                                bool r_too) {
+                                                bool r_too, const float* fl = nullptr) {
     const int64_t o = (rec * P.n + row) * 3;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        if (r_too) P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + (double)f[a]) * P.G.d[a];
+        if (r_too) {
+            const double off = (double)f[a] + (fl ? (double)fl[a] : 0.0);
+            P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + off) * P.G.d[a];
+        }
         P.v_hist[o + a] = (double)vh[a] + (double)vl[a];
     }
 }
@@ -340,7 +393,7 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
             vl[a] = P.fs[(6 + a) * n + s];
         }
         const int64_t row = P.order ? P.order[s] : s;
-        if (RF) c.phase = P.rf_phase[s];
+        if (RF) c.phase = fma(P.omega, P.t0, P.rf_phase[s]);   // omega t0 + phi_i
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
@@ -348,7 +401,10 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
                     // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
                     vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt));
             }
-            if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
+            if (P.r_hist) {
+                const float fl0[3] = {P.fs[9 * n + s], P.fs[10 * n + s], P.fs[11 * n + s]};
+                write_mixed_row(P, 0, row, cell, f, vh, vl, true, fl0);
+            }
         }
         Drift d;
         increment(P, vh, vl, d.dh, d.dl);
@@ -359,20 +415,33 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
         if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
             float cf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
+            float fl[3] = {P.fs[9 * n + s], P.fs[10 * n + s], P.fs[11 * n + s]};
             for (int k = 0; k < nsteps; ++k) {
-                family_step<ALG, RF>(c, cf, f, vh, vl, d, P.step0 + k);
+                family_step<ALG, RF>(c, cf, f, fl, vh, vl, d, P.step0 + k);
                 if (until == 0) {
                     const int64_t rec = (P.step0 + k + 1) / P.rec_every;
                     const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
-                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
+                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true, fl);
                     until = rec_every - 1;
                 } else {
                     --until;
                 }
             }
 #pragma unroll
-            for (int a = 0; a < 3; ++a) cell[a] = (int)cf[a];
+            for (int a = 0; a < 3; ++a) {
+                cell[a] = (int)cf[a];
+                P.fs[(9 + a) * n + s] = fl[a];
+            }
         } else {
+            // these algorithms keep a single float32 offset: fold the low part in
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float x = f[a] + P.fs[(9 + a) * n + s];
+                const float cc = floorf(x);
+                f[a] = fminf(x - cc, kBelowOne);
+                cell[a] += (int)cc;
+                P.fs[(9 + a) * n + s] = 0.0f;
+            }
             for (int k = 0; k < nsteps; ++k) {
                 mixed_step<ALG, RF>(c, cell, f, vh, vl, d, P.step0 + k);
                 if (until == 0) {
@@ -473,6 +542,7 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
     P->dt = a->dt;
     P->t0 = a->t0;
     P->omega = a->rf_omega;
+    P->wdt = a->rf_omega * a->dt;
     P->qm = (float)a->q_over_m;
     P->hqdt = (float)(0.5 * a->q_over_m * a->dt);
     P->dtf = (float)a->dt;

@@ -44,6 +44,7 @@ struct TrackMixDev {
     double dt;
     double t0;
     double omega;
+    double wdt;      // omega dt
     float qm;        // q/m
     float hqdt;      // 0.5 q/m dt
     float dtf;       // dt
