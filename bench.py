@@ -224,11 +224,18 @@ def main():
         half = 0.5 * float(wl.grid[0][-1] - wl.grid[0][0])
         num = torch.linalg.vector_norm(trm.r_hist - r_fp64, dim=2)
         den = torch.clamp(torch.linalg.vector_norm(r_fp64, dim=2), min=half)
-        rel = (num / den).flatten()
+        rel = (num / den).amax(dim=0)          # per particle, worst record
         vrel = (torch.linalg.vector_norm(trm.v_hist - v_fp64, dim=2) /
-                torch.linalg.vector_norm(v_fp64, dim=2)).flatten()
-        err = {"max_rel_pos": float(rel.max()), "p99_rel_pos": float(torch.quantile(rel[:: max(1, rel.numel() // 4_000_000)], 0.99)),
-               "max_rel_vel": float(vrel.max()), "against": "float64 GPU form (pinned to the oracle at 1e-10)"}
+                torch.linalg.vector_norm(v_fp64, dim=2)).amax(dim=0)
+        srt = torch.sort(rel).values
+
+        def q(p):
+            return float(srt[min(srt.numel() - 1, int(p * srt.numel()))])
+
+        err = {"max_rel_pos": float(srt[-1]), "p99_rel_pos": q(0.99), "p99.99_rel_pos": q(0.9999),
+               "particles_over_1e-6": int((rel > 1e-6).sum()), "max_rel_vel": float(vrel.max()),
+               "metric": "per particle max over the 41 snapshots of |r - r64| / max(|r64|, 0.1 m)",
+               "against": "float64 GPU form (pinned to the oracle at 1e-10)"}
         del r_fp64, v_fp64
 
     total_ps = n * wl.nsteps * args.steps * world

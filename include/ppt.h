@@ -130,7 +130,7 @@ int ppt_field_eval(const ppt_fields* fields, int64_t n, const double* pts,
 /* Particle state on the device, structure of arrays:
  *   PPT_PREC_F64:   f64[6*n]  = x | y | z | w_x | w_y | w_z
  *   PPT_PREC_MIXED: i32[3*n]  = cell i | j | k  (on map 0's grid)
- *                   f32[12*n] = offset x|y|z | w_hi x|y|z | w_lo x|y|z | offset_lo x|y|z
+ *                   f32[9*n]  = offset x|y|z | w_hi x|y|z | w_lo x|y|z
  * w is the velocity v [m/s], or u = gamma v for BORIS_REL / VAY. */
 typedef struct {
     int32_t precision;

@@ -70,16 +70,13 @@ __global__ void load_mixed_kernel(int64_t n, const double* __restrict__ r, const
             u = 0.0;
         }
         int cell = (int)fl;
-        double off = u - fl;
-        float f = (float)off;
+        float f = (float)(u - fl);
         if (f >= 1.0f) {
             f = 0.0f;
             cell += 1;
-            off -= 1.0;
         }
         ci[c * n + s] = cell;
         fs[c * n + s] = f;
-        fs[(9 + c) * n + s] = (float)(off - (double)f);   // offset low part
         float hi = (float)vv[c];
         float lo = (float)(vv[c] - (double)hi);
         fs[(3 + c) * n + s] = hi;
@@ -100,9 +97,7 @@ __global__ void store_mixed_kernel(int64_t n, const int32_t* __restrict__ ci, co
         for (int c = 0; c < 3; ++c) w[c] *= ig;
     }
     for (int c = 0; c < 3; ++c) {
-        if (r)
-            r[3 * row + c] =
-                G.lo[c] + ((double)ci[c * n + s] + ((double)fs[c * n + s] + (double)fs[(9 + c) * n + s])) * G.d[c];
+        if (r) r[3 * row + c] = G.lo[c] + ((double)ci[c * n + s] + (double)fs[c * n + s]) * G.d[c];
         if (v) v[3 * row + c] = w[c];
     }
 }

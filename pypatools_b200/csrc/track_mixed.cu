@@ -257,8 +257,8 @@ constexpr float kBelowOne = 0.99999994f;   // largest float below 1
 // such a step is only the position advance: two adds of the float-float
 // increment and a branch-free carry of whole cells.
 template <int ALG, bool RF>
-__device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], float fl[3], float vh[3], float vl[3],
-                                            Drift& d, int64_t g) {
+__device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
+                                            int64_t g) {
     const TrackMixDev& P = *c.P;
     // cheap pre-test on the cell range (the last node layer included); the
     // exact bounds rule is applied inside gather_mixed
@@ -272,26 +272,6 @@ __device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], 
             vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
             increment(P, vh, vl, d.dh, d.dl);
         }
-        // Where fields act, the offset carries its rounding error in fl
-        // (float-float accumulation), so the in-map position does not random-
-        // walk at float32 resolution; that keeps map-exit steps in step with
-        // the float64 form.
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float s = f[a] + d.dh[a];
-            const float bb = s - f[a];
-            float lo = fl[a] + (((f[a] - (s - bb)) + (d.dh[a] - bb)) + d.dl[a]);
-            const float cc = floorf(s);
-            const float sn = s - cc;
-            if (cc < 0.0f) {   // s + |cc| may round: keep that error too (two-sum)
-                const float b2 = sn - s;
-                lo += (s - (sn - b2)) + (-cc - b2);
-            }
-            f[a] = sn;
-            fl[a] = lo;
-            cf[a] += cc;
-        }
-        return;
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -359,18 +339,15 @@ __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], f
     }
 }
 
-// Snapshot row: x = lo + (cell + f + fl) d and v = vh + vl, formed in
-// float64 (output formatting only; fl may be NULL).
+// Snapshot row: x = lo + (cell + f) d and v = vh + vl, formed in float64
+// (output formatting only).
 __device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t rec, int64_t row, const int cell[3],
                                                 const float f[3], const float vh[3], const float vl[3],
-                                                bool r_too, const float* fl = nullptr) {
+                                                bool r_too) {
     const int64_t o = (rec * P.n + row) * 3;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        if (r_too) {
-            const double off = (double)f[a] + (fl ? (double)fl[a] : 0.0);
-            P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + off) * P.G.d[a];
-        }
+        if (r_too) P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + (double)f[a]) * P.G.d[a];
         P.v_hist[o + a] = (double)vh[a] + (double)vl[a];
     }
 }
@@ -401,10 +378,7 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
                     // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
                     vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt));
             }
-            if (P.r_hist) {
-                const float fl0[3] = {P.fs[9 * n + s], P.fs[10 * n + s], P.fs[11 * n + s]};
-                write_mixed_row(P, 0, row, cell, f, vh, vl, true, fl0);
-            }
+            if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
         }
         Drift d;
         increment(P, vh, vl, d.dh, d.dl);
@@ -415,33 +389,20 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
         if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
             float cf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
-            float fl[3] = {P.fs[9 * n + s], P.fs[10 * n + s], P.fs[11 * n + s]};
             for (int k = 0; k < nsteps; ++k) {
-                family_step<ALG, RF>(c, cf, f, fl, vh, vl, d, P.step0 + k);
+                family_step<ALG, RF>(c, cf, f, vh, vl, d, P.step0 + k);
                 if (until == 0) {
                     const int64_t rec = (P.step0 + k + 1) / P.rec_every;
                     const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
-                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true, fl);
+                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
                     until = rec_every - 1;
                 } else {
                     --until;
                 }
             }
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                cell[a] = (int)cf[a];
-                P.fs[(9 + a) * n + s] = fl[a];
-            }
+            for (int a = 0; a < 3; ++a) cell[a] = (int)cf[a];
         } else {
-            // these algorithms keep a single float32 offset: fold the low part in
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const float x = f[a] + P.fs[(9 + a) * n + s];
-                const float cc = floorf(x);
-                f[a] = fminf(x - cc, kBelowOne);
-                cell[a] += (int)cc;
-                P.fs[(9 + a) * n + s] = 0.0f;
-            }
             for (int k = 0; k < nsteps; ++k) {
                 mixed_step<ALG, RF>(c, cell, f, vh, vl, d, P.step0 + k);
                 if (until == 0) {

@@ -107,7 +107,7 @@ class DeviceTracker:
         else:
             self.f64 = None
             self.i32 = torch.empty(3 * n, dtype=torch.int32, device=dev)
-            self.f32 = torch.empty(12 * n, dtype=torch.float32, device=dev)
+            self.f32 = torch.empty(9 * n, dtype=torch.float32, device=dev)
         self.state = _lib.State(_lib.PREC_F64 if precision == "fp64" else _lib.PREC_MIXED,
                                 _lib.ALG_IDS[algorithm], n,
                                 self.f64.data_ptr() if self.f64 is not None else None,
