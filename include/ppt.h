@@ -196,6 +196,19 @@ int64_t ppt_moments_scratch_bytes(int64_t n);
 int ppt_moments(int64_t n, const double* r, const double* v, double mass_mev,
                 double* out, void* scratch, void* stream);
 
+/* ppt_moments without any device allocation, for callers that may not
+ * allocate device memory while they run (an application whose GPU memory is
+ * all owned by another allocator's pool, or an analysis hook inside a
+ * latency-bound loop where cudaMalloc/cudaFree, which can synchronise the
+ * device, are not allowed).  No counterpart in the reference.
+ * Scratch: a static 52 KB device array, held by every GPU that loads the
+ * library until the process exits.  The first call on a device looks up its
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * n must be in [1, 2^53]; anything else returns PPT_ERR_ARG. */
+int ppt_moments_noalloc(int64_t n, const double* r, const double* v, double mass_mev,
+                        double* out, void* stream);
+
 const char* ppt_last_error(void);
 int ppt_abi_version(void);
 

@@ -71,6 +71,7 @@ SIGNATURES = {
     "ppt_cell_sort": (c_int, [POINTER(State), POINTER(Fields), c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_moments_scratch_bytes": (c_int64, [c_int64]),
     "ppt_moments": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
+    "ppt_moments_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p]),
     "ppt_last_error": (ctypes.c_char_p, []),
     "ppt_abi_version": (c_int, []),
 }

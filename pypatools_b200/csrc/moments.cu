@@ -164,3 +164,60 @@ extern "C" int ppt_moments(int64_t n, const double* r, const double* v, double m
     if (!r || !v || !out || !scratch) return fail(PPT_ERR_ARG, "r, v, out and scratch must not be NULL");
     return moments_launch(n, r, v, mass_mev, out, static_cast<double*>(scratch), static_cast<cudaStream_t>(stream));
 }
+
+// ---------------------------------------------------------------------------
+// Moments without any device allocation by the library or the caller.
+//
+// For callers that must not allocate device memory while they run: a host
+// application whose GPU memory is all handed to another allocator's pool, or
+// an analysis hook inside a latency-bound tracking loop, where cudaMalloc /
+// cudaFree (which can synchronise the device) are not allowed.  The scratch
+// lives in a file-scope __device__ array instead; every GPU that loads this
+// library holds it (52 KB) until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace ppt {
+
+// 11 partial sums for each of up to kMomBlocks blocks, then 16 means.
+constexpr int64_t kNoAllocScratchDoubles = (int64_t)kNSum * kMomBlocks + 16;
+static __device__ __align__(256) double g_moments_scratch[kNoAllocScratchDoubles];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_scratch_mutex;
+static double* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_moments_scratch on the current device, looked up once
+// per device (host code only has a host-side stand-in for the symbol).
+static int noalloc_scratch(double** out) {
+    int dev = 0;
+    PPT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(PPT_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_moments_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(moments scratch)");
+        g_scratch_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_addr[dev];
+    return PPT_OK;
+}
+
+}  // namespace ppt
+
+extern "C" int ppt_moments_noalloc(int64_t n, const double* r, const double* v, double mass_mev, double* out,
+                                   void* stream) {
+    if (n <= 0) return fail(PPT_ERR_ARG, "moments need n >= 1");
+    if (n > (1LL << 53))
+        return fail(PPT_ERR_ARG, "ppt_moments_noalloc handles at most 2^53 particles (the float64 count limit)");
+    if (!r || !v || !out) return fail(PPT_ERR_ARG, "r, v and out must not be NULL");
+    if (moments_scratch_doubles() > kNoAllocScratchDoubles)
+        return fail(PPT_ERR_UNSUPPORTED, "moments scratch larger than the static array");
+    double* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    // every partial row and mean the reduction reads is written earlier in the
+    // same call, so nothing in the shared array needs clearing first
+    return moments_launch(n, r, v, mass_mev, out, scratch, static_cast<cudaStream_t>(stream));
+}
