@@ -42,8 +42,43 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--sort-every", type=int, default=500)
+    ap.add_argument("--sort-every", type=int, default=100,
+                    help="cell re-sort interval in steps (also the launch length); 0 = never")
+    ap.add_argument("--serve-jobs", type=int, default=300,
+                    help="jobs of the serving stream per form (2000 = the full stream); 0 skips it")
     return ap.parse_args()
+
+
+def run_serving(n_jobs, device, rate=50.0):
+    """The serving stream (Poisson arrivals at 50 jobs/s, 1e3-1e6 protons,
+    Boris / Vay / RK4, 1000-10000 steps, 4 resident float32 maps 64^3-256^3,
+    120 GB admission budget) in real time, mixed then float64."""
+    import torch
+    from pypatools_b200 import Field, IonSpecies, workloads
+    from pypatools_b200.serving import TrackingJob, TrackingServer
+
+    ion = IonSpecies("proton")
+    fields = []
+    for grid, e, b in workloads.serving_maps():
+        g = {"x": grid[0], "y": grid[1], "z": grid[2]}
+        fields.append((Field.zero(3) if e is None else Field.from_arrays(g, e), Field.from_arrays(g, b)))
+    specs = workloads.serving_stream(n_jobs=n_jobs, rate=rate)
+    warm = workloads.serving_stream(n_jobs=12, rate=rate, seed=40, n_max=1e4, steps_max=1500)
+    out = {}
+    for form in ("mixed", "fp64"):
+        def jobs_of(sp):
+            return [TrackingJob(s.job_id, ion.q_over_m, s.algorithm, s.r0, s.v0, *fields[s.map_index], s.nsteps,
+                                1e-11, precision=form, arrival=s.arrival) for s in sp]
+        TrackingServer(device=device, chunk=500).run(jobs_of(warm), realtime=False)   # kernels, graphs, maps
+        server = TrackingServer(device=device, budget_bytes=120e9, chunk=500)
+        rep = server.run(jobs_of(specs), realtime=True)
+        span = specs[-1].arrival
+        rep["offered_particle_steps_per_s"] = sum(s.n * s.nsteps for s in specs) / span if span > 0 else None
+        out[form] = rep
+        torch.cuda.synchronize()
+    return {"stream": f"{n_jobs} jobs, Poisson {rate}/s, 1e3-1e6 protons, boris/vay_rel/rk4_rel, "
+                      "1000-10000 steps, maps 64^3/128^3/192^3/256^3 float32, 120 GB budget, chunk 500",
+            "mixed": out["mixed"], "fp64": out["fp64"]}
 
 
 # ---------------------------------------------------------------------------
@@ -108,6 +143,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def max_over_ranks(value, world, device):
+    """The slowest rank's device time: replicas report the job as done when
+    the last one is (the only collective on the bench path)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return
@@ -149,7 +196,7 @@ def main():
     d_r0 = torch.from_numpy(wl.r0).to(dev)
     d_v0 = torch.from_numpy(wl.v0).to(dev)
     d_phase = torch.from_numpy(wl.rf_phase).to(dev)
-    chunk = wl.rec_every
+    chunk = min(wl.rec_every, args.sort_every) if args.sort_every > 0 else wl.rec_every
     n = wl.n
 
     def run_form(precision):
@@ -194,11 +241,7 @@ def main():
         t1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = t0.elapsed_time(t1)
-        if world > 1:
-            tt = torch.tensor([ms], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
+        ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
         cnt = tr.counter_values()
         launch_ms = [a.elapsed_time(b) for a, b in launch_ev]
         out = {"ms_total": ms, "ms_per_job": ms / args.steps, "launch_ms": launch_ms,
@@ -284,6 +327,11 @@ def main():
                "api": "PusherGPU.track_batch (numpy in, numpy histories out)", "steps": args.e2e_steps}
         del rh, vh
 
+    serving = None
+    if args.serve_jobs > 0:
+        torch.cuda.empty_cache()
+        serving = run_serving(args.serve_jobs, dev)
+
     cpu = None
     if rank == 0:
         from oracle import cpu_baseline
@@ -311,6 +359,7 @@ def main():
             "e2e": e2e,
             "gpu_launches": m["launches"],
             "clocks": clocks,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

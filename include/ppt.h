@@ -175,6 +175,46 @@ typedef struct {
  * v_hist at the reference's record indices. */
 int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_track_args* args, void* stream);
 
+/* ---- serving: many jobs per launch -------------------------------------
+ * No reference counterpart (the reference runs one track_batch at a time,
+ * pusher.py:894-1012).  A job is one track_batch call's device state. */
+typedef struct {
+    ppt_state state;          /* the job's particle state (loaded with ppt_state_load) */
+    ppt_fields fields;
+    int64_t nsteps_total;
+    int64_t rec_every;
+    double dt;
+    double q_over_m;
+    double t0;
+    double rf_omega;
+    const double* rf_phase;   /* device float64 [n] or NULL */
+    double* r_hist;           /* device (nsteps_total/rec_every + 1, n, 3) or NULL */
+    double* v_hist;
+    int32_t* status;          /* device int32 or NULL */
+    int64_t steps_done;       /* steps already taken (a table rebuilt mid-track resumes here) */
+} ppt_job_desc;
+
+typedef struct ppt_jobs ppt_jobs;   /* opaque host handle */
+
+/* Device bytes ppt_jobs_create needs for n_jobs jobs. */
+int64_t ppt_jobs_scratch_bytes(int n_jobs);
+
+/* Write the job table into scratch (device, ppt_jobs_scratch_bytes bytes;
+ * caller-owned, must outlive the handle) with every job at step 0.  The
+ * descriptors' device buffers must outlive the handle too. */
+int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scratch, ppt_jobs** out, void* stream);
+
+/* Advance every unfinished job by up to chunk steps (Boris-family half steps
+ * and snapshots exactly as ppt_track).  Reads no host data and does not
+ * synchronise: a captured CUDA graph of this call can be replayed. */
+int ppt_jobs_tick(ppt_jobs* jobs, int64_t chunk, void* stream);
+
+/* Device pointers to the per-job steps done (int64[n_jobs]) and done flags
+ * (int32[n_jobs], 1 once a job's last step ran). */
+int ppt_jobs_progress(const ppt_jobs* jobs, int64_t** steps, int32_t** done);
+
+int ppt_jobs_destroy(ppt_jobs* jobs);
+
 /* Reorder particles by cell (locality of the corner gathers).  Permutes the
  * state, rf_phase and order arrays in place.  Needs n_cells_hint >= 1.
  * scratch: device buffer of ppt_cell_sort_scratch_bytes(n) bytes. */

@@ -57,6 +57,13 @@ class TrackArgs(ctypes.Structure):
                 ("counters", c_void_p)]
 
 
+class JobDesc(ctypes.Structure):
+    _fields_ = [("state", State), ("fields", Fields), ("nsteps_total", c_int64), ("rec_every", c_int64),
+                ("dt", c_double), ("q_over_m", c_double), ("t0", c_double), ("rf_omega", c_double),
+                ("rf_phase", c_void_p), ("r_hist", c_void_p), ("v_hist", c_void_p), ("status", c_void_p),
+                ("steps_done", c_int64)]
+
+
 # name -> (restype, argtypes); every symbol include/ppt.h declares
 SIGNATURES = {
     "ppt_fieldmap_create": (c_int, [POINTER(GridDesc), c_int, c_int, c_int, POINTER(c_void_p)]),
@@ -72,6 +79,11 @@ SIGNATURES = {
     "ppt_moments_scratch_bytes": (c_int64, [c_int64]),
     "ppt_moments": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "ppt_moments_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p]),
+    "ppt_jobs_scratch_bytes": (c_int64, [c_int]),
+    "ppt_jobs_create": (c_int, [POINTER(JobDesc), c_int, c_void_p, POINTER(c_void_p), c_void_p]),
+    "ppt_jobs_tick": (c_int, [c_void_p, c_int64, c_void_p]),
+    "ppt_jobs_progress": (c_int, [c_void_p, POINTER(c_void_p), POINTER(c_void_p)]),
+    "ppt_jobs_destroy": (c_int, [c_void_p]),
     "ppt_last_error": (ctypes.c_char_p, []),
     "ppt_abi_version": (c_int, []),
 }

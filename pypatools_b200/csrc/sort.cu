@@ -41,37 +41,52 @@ __device__ __forceinline__ uint32_t bucket_of_cells(const SortGeom& G, int c0, i
     return (uint32_t)(lin % G.n_in);
 }
 
-// Histogram + in-map count with one atomic per distinct key per warp.
+// Histogram of the in-map keys (one atomic per distinct key per warp) and the
+// in-map count (one atomic per block).  Particles outside the map touch no
+// counter: their bucket's size is n minus the in-map count, filled in by the
+// scan, so a bunch that has left the map costs no same-address atomics.
 __device__ __forceinline__ void count_key(uint32_t b, bool inside, uint32_t* count, uint32_t* ctrl) {
-    const unsigned active = __activemask();
-    const unsigned same = __match_any_sync(active, b);
-    const int lane = threadIdx.x & 31;
-    if (lane == __ffs(same) - 1) atomicAdd(count + b, (uint32_t)__popc(same));
-    const unsigned in_mask = __ballot_sync(active, inside);
-    if (lane == __ffs(active) - 1 && in_mask) atomicAdd(ctrl, (uint32_t)__popc(in_mask));
+    __shared__ unsigned block_in;
+    if (threadIdx.x == 0) block_in = 0;
+    __syncthreads();
+    if (inside) {
+        const unsigned active = __activemask();
+        const unsigned same = __match_any_sync(active, b);
+        const int lane = threadIdx.x & 31;
+        if (lane == __ffs(same) - 1) {
+            atomicAdd(count + b, (uint32_t)__popc(same));
+            atomicAdd(&block_in, (unsigned)__popc(same));
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && block_in) atomicAdd(ctrl, block_in);
 }
 
 __global__ void sort_keys_f64(int64_t n, const double* __restrict__ st, SortGeom G, uint32_t* __restrict__ key,
                               uint32_t* __restrict__ count, uint32_t* __restrict__ ctrl) {
-    int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    int c[3];
-    for (int a = 0; a < 3; ++a) {
-        double u = (st[a * n + s] - G.lo[a]) * G.inv_d[a];
-        c[a] = (u >= 0.0 && u < 2.0e9) ? (int)u : -1;
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    uint32_t b = G.outside;
+    if (s < n) {
+        int c[3];
+        for (int a = 0; a < 3; ++a) {
+            double u = (st[a * n + s] - G.lo[a]) * G.inv_d[a];
+            c[a] = (u >= 0.0 && u < 2.0e9) ? (int)u : -1;
+        }
+        b = bucket_of_cells(G, c[0], c[1], c[2]);
+        key[s] = b;
     }
-    uint32_t b = bucket_of_cells(G, c[0], c[1], c[2]);
-    key[s] = b;
-    count_key(b, b != G.outside, count, ctrl);
+    count_key(b, s < n && b != G.outside, count, ctrl);
 }
 
 __global__ void sort_keys_mixed(int64_t n, const int32_t* __restrict__ ci, SortGeom G, uint32_t* __restrict__ key,
                                 uint32_t* __restrict__ count, uint32_t* __restrict__ ctrl) {
-    int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    uint32_t b = bucket_of_cells(G, ci[s], ci[n + s], ci[2 * n + s]);
-    key[s] = b;
-    count_key(b, b != G.outside, count, ctrl);
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    uint32_t b = G.outside;
+    if (s < n) {
+        b = bucket_of_cells(G, ci[s], ci[n + s], ci[2 * n + s]);
+        key[s] = b;
+    }
+    count_key(b, s < n && b != G.outside, count, ctrl);
 }
 
 __device__ __forceinline__ bool sort_wanted(const uint32_t* ctrl, int64_t n) {
@@ -110,6 +125,7 @@ __global__ void __launch_bounds__(kScanTile) scan_tiles(int64_t nb, const uint32
     __shared__ uint32_t sh[32];
     int64_t i = blockIdx.x * (int64_t)kScanTile + threadIdx.x;
     uint32_t v = i < nb ? count[i] : 0u;
+    if (i == nb - 1) v = (uint32_t)(n - (int64_t)ctrl[0]);   // the outside bucket: everything not in the map
     uint32_t total;
     uint32_t ex = block_exclusive_scan(v, sh, total);
     if (i < nb) offset[i] = ex;

@@ -238,13 +238,14 @@ __device__ __forceinline__ void add_counters(unsigned long long* counters, unsig
     }
 }
 
+__device__ __forceinline__ Ctx make_ctx(const TrackDev& P) {
+    return Ctx{&P.F, P.dt, P.qm, P.omega, 0.0, P.t0, 0u, P.F.e_const_nz | P.F.b_const_nz};
+}
+
+// All steps of one call for particle slot s (s < P.n); returns the steps done.
 template <int ALG, bool RF>
-__global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ TrackDev P) {
-    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool live = s < P.n;
-    unsigned steps_done = 0;
-    Ctx c{&P.F, P.dt, P.qm, P.omega, 0.0, P.t0, 0u, P.F.e_const_nz | P.F.b_const_nz};
-    if (live) {
+__device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_t s, Ctx& c) {
+    {
         const int64_t n = P.n;
         double* st = P.f64;
         V3 r = v3(st[s], st[n + s], st[2 * n + s]);
@@ -268,20 +269,25 @@ __global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ 
         const int rec_every = P.rec_every > 0x7fffffff ? 0x7fffffff : (int)P.rec_every;
         const int64_t until64 = P.rec_every - 1 - (P.step0 % P.rec_every);
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
-        for (int k = 0; k < nsteps; ++k) {
-            step<ALG, RF>(c, r, w, P.step0 + k);
-            if (until == 0) {
-                const int64_t rec = (P.step0 + k + 1) / P.rec_every;
+        // record-free segments: the inner loop carries only its counter
+        int k = 0;
+        while (k < nsteps) {
+            const int64_t to_rec = (int64_t)until + 1;
+            const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
+            const int64_t g0 = P.step0 + k;
+            for (int i = 0; i < seg; ++i) step<ALG, RF>(c, r, w, g0 + i);
+            k += seg;
+            if ((int64_t)seg == to_rec) {
+                const int64_t rec = (P.step0 + k) / P.rec_every;
                 if (P.r_hist && rec < P.n_rec) {
                     write_row(P.r_hist, rec, n, row, r);
                     write_row(P.v_hist, rec, n, row, w_to_v<ALG>(w));
                 }
                 until = rec_every - 1;
             } else {
-                --until;
+                until -= seg;
             }
         }
-        steps_done = (unsigned)P.nsteps;
         if (P.flags & PPT_TRACK_FINAL) {
             if constexpr (alg_staggered(ALG)) {
                 V3 E, B;
@@ -301,7 +307,84 @@ __global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ 
             if (!isfinite(sum)) atomicOr(P.status, PPT_STATUS_NONFINITE);
         }
     }
+    return (unsigned)P.nsteps;
+}
+
+template <int ALG, bool RF>
+__global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ TrackDev P) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned steps_done = 0;
+    Ctx c = make_ctx(P);
+    if (s < P.n) steps_done = track_f64_particle<ALG, RF>(P, s, c);
     if (P.counters) add_counters(P.counters, c.hits, steps_done);
+}
+
+// Serving: a persistent block-level work queue over the float64 jobs of one
+// (algorithm, RF) class.  Each item is one job's 128-particle block; the job's
+// parameter block is staged in shared memory and its step window for this
+// tick comes from the device-resident step counters.
+static_assert(sizeof(TrackDev) % 8 == 0, "TrackDev is copied as 8-byte words");
+
+template <int ALG, bool RF>
+__global__ void __launch_bounds__(kJobBlock) track_f64_jobs_kernel(const __grid_constant__ JobQueueDev Q) {
+    __shared__ __align__(16) TrackDev sP;
+    __shared__ int s_item, s_job;
+    const TrackDev* table = static_cast<const TrackDev*>(Q.table);
+    for (;;) {
+        take_item(Q, &s_item, &s_job);
+        const int it = s_item;
+        if (it >= Q.n_items) return;
+        const int cj = s_job;
+        const int gjob = Q.job_index[cj];
+        {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(table + Q.table_index[cj]);
+            uint64_t* dst = reinterpret_cast<uint64_t*>(&sP);
+            for (int i = threadIdx.x; i < (int)(sizeof(TrackDev) / 8); i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t s0, k;
+            int fl;
+            job_window(Q, gjob, sP.nsteps_total, &s0, &k, &fl);
+            sP.step0 = s0;
+            sP.nsteps = k;
+            sP.flags = Q.done[gjob] ? -1 : fl;   // -1: job finished, nothing to do
+        }
+        __syncthreads();
+        if (sP.flags >= 0) {
+            const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
+            Ctx c = make_ctx(sP);
+            unsigned sd = 0;
+            if (s < sP.n) sd = track_f64_particle<ALG, RF>(sP, s, c);
+            if (sP.counters) add_counters(sP.counters, c.hits, sd);
+        }
+        __syncthreads();
+    }
+}
+
+template <int ALG>
+static cudaError_t launch_jobs_alg(const JobQueueDev& Q, bool rf, int grid, cudaStream_t s) {
+    if (rf) track_f64_jobs_kernel<ALG, true><<<grid, kJobBlock, 0, s>>>(Q);
+    else track_f64_jobs_kernel<ALG, false><<<grid, kJobBlock, 0, s>>>(Q);
+    return cudaGetLastError();
+}
+
+int launch_f64_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s) {
+    cudaError_t e;
+    switch (algorithm) {
+        case PPT_ALG_LEAPFROG: e = launch_jobs_alg<PPT_ALG_LEAPFROG>(Q, rf, grid, s); break;
+        case PPT_ALG_BORIS: e = launch_jobs_alg<PPT_ALG_BORIS>(Q, rf, grid, s); break;
+        case PPT_ALG_RK4: e = launch_jobs_alg<PPT_ALG_RK4>(Q, rf, grid, s); break;
+        case PPT_ALG_YOSHIDA: e = launch_jobs_alg<PPT_ALG_YOSHIDA>(Q, rf, grid, s); break;
+        case PPT_ALG_VAY_REL: e = launch_jobs_alg<PPT_ALG_VAY_REL>(Q, rf, grid, s); break;
+        case PPT_ALG_RK4_REL: e = launch_jobs_alg<PPT_ALG_RK4_REL>(Q, rf, grid, s); break;
+        case PPT_ALG_YOSHIDA_REL: e = launch_jobs_alg<PPT_ALG_YOSHIDA_REL>(Q, rf, grid, s); break;
+        case PPT_ALG_BORIS_REL: e = launch_jobs_alg<PPT_ALG_BORIS_REL>(Q, rf, grid, s); break;
+        case PPT_ALG_VAY: e = launch_jobs_alg<PPT_ALG_VAY>(Q, rf, grid, s); break;
+        default: return fail(PPT_ERR_ARG, "unknown algorithm");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "track_f64_jobs_kernel launch");
+    return PPT_OK;
 }
 
 template <int ALG>

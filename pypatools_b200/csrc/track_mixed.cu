@@ -133,7 +133,9 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
             double ph = fma((double)g, c.P->wdt, c.phase);
             if (toff != 0.0) ph = fma(c.P->omega, toff, ph);
             double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
-            float cf = cosf((float)red);
+            // the argument is already in [-pi, pi], where the hardware cosine's
+            // absolute error (2^-21.4) is below the float32 field values' own
+            float cf = __cosf((float)red);
             E = cf * E;
         }
     }
@@ -249,8 +251,6 @@ struct Drift {
     bool inside;
 };
 
-constexpr float kBelowOne = 0.99999994f;   // largest float below 1
-
 // One step of the Boris family (Boris, leapfrog) with float-valued cell
 // indices (exact integers below 2^24).  Outside the map with no constant
 // field both updates leave v exactly unchanged (every added term is zero), so
@@ -272,13 +272,24 @@ __device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], 
             vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
             increment(P, vh, vl, d.dh, d.dl);
         }
+        // where fields act, the full float-float increment
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float x = f[a] + d.dh[a];
+            x = x + d.dl[a];
+            const float cc = floorf(x);
+            f[a] = x - cc;   // in [0, 1]: 1 only for x a hair below an integer, the same point as (cc + 1, 0)
+            cf[a] += cc;
+        }
+        return;
     }
+    // Drift: no field acts, so the low part of the increment (a 3e-8 relative
+    // correction of the displacement) is left out.
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float x = f[a] + d.dh[a];
-        x = x + d.dl[a];
+        const float x = f[a] + d.dh[a];
         const float cc = floorf(x);
-        f[a] = fminf(x - cc, kBelowOne);   // x - floor(x) rounds to 1 only for x just below an integer
+        f[a] = x - cc;
         cf[a] += cc;
     }
 }
@@ -353,12 +364,8 @@ __device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t re
 }
 
 template <int ALG, bool RF>
-__global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
-    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool live = s < P.n;
-    unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u};
-    if (live) {
+__device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, int64_t s, MixCtx& c) {
+    {
         const int64_t n = P.n;
         int cell[3];
         float f[3], vh[3], vl[3];
@@ -389,15 +396,21 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
         if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
             float cf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
-            for (int k = 0; k < nsteps; ++k) {
-                family_step<ALG, RF>(c, cf, f, vh, vl, d, P.step0 + k);
-                if (until == 0) {
-                    const int64_t rec = (P.step0 + k + 1) / P.rec_every;
+            // record-free segments: the inner loop carries only its counter
+            int k = 0;
+            while (k < nsteps) {
+                const int64_t to_rec = (int64_t)until + 1;
+                const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
+                const int64_t g0 = P.step0 + k;
+                for (int i = 0; i < seg; ++i) family_step<ALG, RF>(c, cf, f, vh, vl, d, g0 + i);
+                k += seg;
+                if ((int64_t)seg == to_rec) {
+                    const int64_t rec = (P.step0 + k) / P.rec_every;
                     const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
                     if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
                     until = rec_every - 1;
                 } else {
-                    --until;
+                    until -= seg;
                 }
             }
 #pragma unroll
@@ -414,7 +427,6 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
                 }
             }
         }
-        steps_done = (unsigned)P.nsteps;
         if (P.flags & PPT_TRACK_FINAL) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
@@ -438,18 +450,92 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
             if (abs(cell[0]) >= lim || abs(cell[1]) >= lim || abs(cell[2]) >= lim) atomicOr(P.status, PPT_STATUS_RANGE);
         }
     }
-    if (P.counters) {
-        unsigned long long h = c.hits, st = steps_done;
+    return (unsigned)P.nsteps;
+}
+
+__device__ __forceinline__ void add_mixed_counters(unsigned long long* counters, unsigned hits, unsigned steps) {
+    unsigned long long h = hits, st = steps;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            h += __shfl_down_sync(0xffffffffu, h, o);
-            st += __shfl_down_sync(0xffffffffu, st, o);
-        }
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(P.counters, h);
-            atomicAdd(P.counters + 1, st);
-        }
+    for (int o = 16; o > 0; o >>= 1) {
+        h += __shfl_down_sync(0xffffffffu, h, o);
+        st += __shfl_down_sync(0xffffffffu, st, o);
     }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters, h);
+        atomicAdd(counters + 1, st);
+    }
+}
+
+template <int ALG, bool RF>
+__global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned steps_done = 0;
+    MixCtx c{&P, 0.0, 0u};
+    if (s < P.n) steps_done = track_mixed_particle<ALG, RF>(P, s, c);
+    if (P.counters) add_mixed_counters(P.counters, c.hits, steps_done);
+}
+
+// Serving: the mixed-precision counterpart of track_f64_jobs_kernel.
+static_assert(sizeof(TrackMixDev) % 8 == 0, "TrackMixDev is copied as 8-byte words");
+
+template <int ALG, bool RF>
+__global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __grid_constant__ JobQueueDev Q) {
+    __shared__ __align__(16) TrackMixDev sP;
+    __shared__ int s_item, s_job;
+    const TrackMixDev* table = static_cast<const TrackMixDev*>(Q.table);
+    for (;;) {
+        take_item(Q, &s_item, &s_job);
+        const int it = s_item;
+        if (it >= Q.n_items) return;
+        const int cj = s_job;
+        const int gjob = Q.job_index[cj];
+        {
+            const uint64_t* src = reinterpret_cast<const uint64_t*>(table + Q.table_index[cj]);
+            uint64_t* dst = reinterpret_cast<uint64_t*>(&sP);
+            for (int i = threadIdx.x; i < (int)(sizeof(TrackMixDev) / 8); i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int64_t s0, k;
+            int fl;
+            job_window(Q, gjob, sP.nsteps_total, &s0, &k, &fl);
+            sP.step0 = s0;
+            sP.nsteps = k;
+            sP.flags = Q.done[gjob] ? -1 : fl;
+        }
+        __syncthreads();
+        if (sP.flags >= 0) {
+            const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
+            MixCtx c{&sP, 0.0, 0u};
+            unsigned sd = 0;
+            if (s < sP.n) sd = track_mixed_particle<ALG, RF>(sP, s, c);
+            if (sP.counters) add_mixed_counters(sP.counters, c.hits, sd);
+        }
+        __syncthreads();
+    }
+}
+
+template <int ALG>
+static cudaError_t launch_mixed_jobs_alg(const JobQueueDev& Q, bool rf, int grid, cudaStream_t s) {
+    if (rf) track_mixed_jobs_kernel<ALG, true><<<grid, kJobBlock, 0, s>>>(Q);
+    else track_mixed_jobs_kernel<ALG, false><<<grid, kJobBlock, 0, s>>>(Q);
+    return cudaGetLastError();
+}
+
+int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s) {
+    cudaError_t e;
+    switch (algorithm) {
+        case PPT_ALG_LEAPFROG: e = launch_mixed_jobs_alg<PPT_ALG_LEAPFROG>(Q, rf, grid, s); break;
+        case PPT_ALG_BORIS: e = launch_mixed_jobs_alg<PPT_ALG_BORIS>(Q, rf, grid, s); break;
+        case PPT_ALG_RK4: e = launch_mixed_jobs_alg<PPT_ALG_RK4>(Q, rf, grid, s); break;
+        case PPT_ALG_VAY_REL: e = launch_mixed_jobs_alg<PPT_ALG_VAY_REL>(Q, rf, grid, s); break;
+        case PPT_ALG_RK4_REL: e = launch_mixed_jobs_alg<PPT_ALG_RK4_REL>(Q, rf, grid, s); break;
+        default:
+            return fail(PPT_ERR_UNSUPPORTED,
+                        "the mixed form covers leapfrog, boris, rk4, vay_rel and rk4_rel; use precision 'fp64'");
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "track_mixed_jobs_kernel launch");
+    return PPT_OK;
 }
 
 template <int ALG>

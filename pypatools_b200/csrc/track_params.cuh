@@ -62,11 +62,62 @@ struct TrackMixDev {
     unsigned long long* counters;
 };
 
+// One (form, algorithm, RF) class of serving jobs: a block-level work queue
+// over items = (job, 128-particle block) pairs.  The job tables, the per-job
+// step counters and done flags live in device memory, so a tick needs no
+// host data and can be replayed from a captured CUDA graph.
+struct JobQueueDev {
+    const void* table;        // TrackDev[] (float64 jobs) or TrackMixDev[] (mixed jobs), by table index
+    const int* table_index;   // class-local job -> table index
+    const int* job_index;     // class-local job -> global job index (steps / done)
+    const int* item_start;    // class-local prefix sums of items, n_jobs + 1 entries
+    int n_jobs;
+    int n_items;
+    unsigned* queue;          // work-queue head, zeroed before each tick
+    const int64_t* steps;     // steps done per global job
+    const int* done;          // 1 once the job's last step ran
+    int64_t chunk;            // steps per tick
+};
+
+constexpr int kJobBlock = 128;
+
 int mixed_grid(const FieldsDev& F, GridF* G);
 int check_state(const ppt_state* st);
 int launch_track_f64(const TrackDev& P, int algorithm, bool rf, cudaStream_t s);
 int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_args* a, int64_t n_rec,
                      TrackMixDev* P);
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s);
+int launch_f64_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s);
+int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s);
+
+// Device helper shared by both job kernels: thread 0 takes the next item and
+// finds its class-local job by bisection over item_start.
+__device__ __forceinline__ void take_item(const JobQueueDev& Q, int* s_item, int* s_job) {
+    if (threadIdx.x == 0) {
+        const int it = (int)atomicAdd(Q.queue, 1u);
+        int lo = 0, hi = Q.n_jobs;   // item_start[lo] <= it < item_start[hi]
+        if (it < Q.n_items) {
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (Q.item_start[mid] <= it) lo = mid; else hi = mid;
+            }
+        }
+        *s_item = it;
+        *s_job = lo;
+    }
+    __syncthreads();
+}
+
+// Step window of a job in this tick: [step0, step0 + k) and its flags.
+__device__ __forceinline__ void job_window(const JobQueueDev& Q, int gjob, int64_t total, int64_t* step0,
+                                           int64_t* k, int* flags) {
+    const int64_t s0 = Q.steps[gjob];
+    int64_t kk = total - s0;
+    if (kk > Q.chunk) kk = Q.chunk;
+    if (kk < 0) kk = 0;
+    *step0 = s0;
+    *k = kk;
+    *flags = (s0 == 0 ? PPT_TRACK_INIT : 0) | (s0 + kk == total ? PPT_TRACK_FINAL : 0);
+}
 
 }  // namespace ppt

@@ -77,6 +77,23 @@ def _interp_grid_values(interp):
     return tuple(np.asarray(g, dtype=np.float64) for g in grid), values
 
 
+_zero_cache = {}
+
+
+def _all_zero(values):
+    """True when a node array is identically zero; remembered per buffer
+    (address, shape, dtype) so repeated cache lookups do not rescan maps."""
+    a = np.asarray(values)
+    key = (a.__array_interface__["data"][0], a.shape, a.dtype.str)
+    hit = _zero_cache.get(key)
+    if hit is None:
+        hit = not np.any(a)
+        if len(_zero_cache) > 4096:
+            _zero_cache.clear()
+        _zero_cache[key] = hit
+    return hit
+
+
 def decompose(field):
     """Field-like object -> FieldTerms."""
     out = FieldTerms()
@@ -119,7 +136,7 @@ def decompose(field):
         if grid is None:
             return out
         # Field.zero(): all-zero node values contribute nothing anywhere
-        if all(values[c] is None or not np.any(values[c]) for c in "xyz"):
+        if all(values[c] is None or _all_zero(values[c]) for c in "xyz"):
             return out
         out.terms.append(_MapTerm(grid, values, scaling))
         return out

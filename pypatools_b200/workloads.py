@@ -176,3 +176,50 @@ def sector_ring_protons(n=100_000_000, nsteps=50_000, seed=5, nodes=512, rec_eve
     return Workload("sector_ring_protons", ion, r0, v0, (g, g.copy(), g.copy()), None, b,
                     dt=1e-10, nsteps=nsteps, rec_every=rec_every or nsteps,
                     meta={"r_eq": r_eq})
+
+
+def serving_maps(map_dtype=np.float32):
+    """The 4 resident maps of the serving stream: 64^3 quadrupole-solenoid B
+    (+-5 cm), 128^3 radial E + solenoid B (+-10 cm), 192^3 and 256^3 RF-gap
+    Ez + Bz (+-10 cm, static).  Returns [(grid, e_values, b_values), ...]."""
+    out = []
+    q = quad_solenoid_protons(n=1, nsteps=1, nodes=64)
+    out.append((q.grid, None, {c: q.b_values[c].astype(map_dtype) for c in "xyz"}))
+    r = radial_e_solenoid_electrons(n=1, nsteps=1, nodes=128, map_dtype=map_dtype)
+    out.append((r.grid, r.e_values, r.b_values))
+    for nodes in (192, 256):
+        g = rf_gap_protons(n=1, nsteps=1, nodes=nodes, map_dtype=map_dtype)
+        out.append((g.grid, g.e_values, g.b_values))
+    return out
+
+
+@dataclass
+class ServingJobSpec:
+    job_id: int
+    arrival: float
+    n: int
+    algorithm: str
+    nsteps: int
+    map_index: int
+    r0: np.ndarray
+    v0: np.ndarray
+
+
+def serving_stream(n_jobs=2000, rate=50.0, seed=4, n_min=1e3, n_max=1e6, steps_min=1000, steps_max=10000,
+                   algorithms=("boris", "vay_rel", "rk4_rel"), n_maps=4):
+    """Poisson arrivals at ``rate`` jobs/s; particle counts log-uniform in
+    [n_min, n_max]; pusher uniform over ``algorithms``; step counts uniform
+    in [steps_min, steps_max]; map uniform over the resident maps; each bunch
+    drawn like the quadrupole-solenoid protons with seed 1000 + job_id."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_jobs)).astype(np.int64)
+    algs = rng.integers(0, len(algorithms), n_jobs)
+    steps = rng.integers(steps_min, steps_max + 1, n_jobs)
+    maps = rng.integers(0, n_maps, n_jobs)
+    specs = []
+    for j in range(n_jobs):
+        b = quad_solenoid_protons(n=int(ns[j]), nsteps=int(steps[j]), seed=1000 + j, nodes=2)
+        specs.append(ServingJobSpec(j, float(arrivals[j]), int(ns[j]), algorithms[int(algs[j])], int(steps[j]),
+                                    int(maps[j]), b.r0, b.v0))
+    return specs
