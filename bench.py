@@ -49,6 +49,12 @@ def parse():
     return ap.parse_args()
 
 
+# DRAM bytes per particle per launch of the mixed track kernel, from the ncu
+# capture of a 100-step in-map launch on the RF-gap workload at 1e6 protons
+# (the state read and written; the map's occupied cells stay in L2).
+MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 66.5
+
+
 def run_serving(n_jobs, device, rate=50.0):
     """The serving stream (Poisson arrivals at 50 jobs/s, 1e3-1e6 protons,
     Boris / Vay / RK4, 1000-10000 steps, 4 resident float32 maps 64^3-256^3,
@@ -298,7 +304,11 @@ def main():
     avg_launch_s = float(np.mean(m["launch_ms"])) / 1e3
     achieved = alg_bytes_per_launch / avg_launch_s / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs",
+                "traffic": MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH * n,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one in-map 100-step launch "
+                                  "at 1e6 protons (profiles/track_mixed_kernel_rf_gap_1e6_in_map.txt), scaled "
+                                  "by particle count; the gathers are served from L1/L2",
+                "peak_kind": f"{peak_kind} hbm_gbs",
                 "kernel": "track_mixed_kernel<BORIS,RF>", "avg_launch_ms": avg_launch_s * 1e3,
                 "in_map_fraction": hits / max(1, m["counters"]["particle_steps"]),
                 "note": "gathers only for in-map particle-steps; the rest are register-only drift steps"}

@@ -54,6 +54,14 @@ int build_fields(const ppt_fields* f, FieldsDev* out) {
         out->e_maps += out->maps[i].has_e;
         out->b_maps += out->maps[i].has_b;
     }
+    for (int a = 0; a < 3; ++a) {
+        out->box_lo[a] = f->n_maps ? out->maps[0].ax[a].lo : 0.0;
+        out->box_hi[a] = f->n_maps ? out->maps[0].ax[a].hi : 0.0;
+        for (int i = 1; i < f->n_maps; ++i) {
+            out->box_lo[a] = std::min(out->box_lo[a], out->maps[i].ax[a].lo);
+            out->box_hi[a] = std::max(out->box_hi[a], out->maps[i].ax[a].hi);
+        }
+    }
     for (int c = 0; c < 3; ++c) {
         out->e_const[c] = f->e_const[c];
         out->b_const[c] = f->b_const[c];

@@ -83,6 +83,8 @@ struct FieldsDev {
     int b_const_nz;
     double e_const[3];
     double b_const[3];
+    double box_lo[3];   // union of the maps' node boxes: a point outside it is outside every map
+    double box_hi[3];
 };
 
 int build_fields(const ppt_fields* f, FieldsDev* out);
@@ -157,8 +159,12 @@ struct Cell {
     double tx, ty, tz;
 };
 
+__device__ __forceinline__ bool axis_contains(const AxisDev& a, double x) { return x >= a.lo && x <= a.hi; }
+
 __device__ __forceinline__ bool locate(const MapDev& m, V3 r, Cell& c) {
     int i, j, k;
+    // the three bounds tests first: a point outside on any axis costs no cell search
+    if (!(axis_contains(m.ax[0], r.x) & axis_contains(m.ax[1], r.y) & axis_contains(m.ax[2], r.z))) return false;
     if (!locate_axis(m.ax[0], r.x, i, c.tx)) return false;
     if (!locate_axis(m.ax[1], r.y, j, c.ty)) return false;
     if (!locate_axis(m.ax[2], r.z, k, c.tz)) return false;

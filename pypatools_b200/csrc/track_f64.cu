@@ -157,8 +157,51 @@ __device__ __forceinline__ int fields_at(Ctx& c, V3 r, int64_t g, double toff, V
     return h;
 }
 
+// Position advance of one step, r + v dt (pusher.py:395-404).
+__device__ __forceinline__ V3 drift(V3 r, V3 v, double dt) {
+    return v3(fma(v.x, dt, r.x), fma(v.y, dt, r.y), fma(v.z, dt, r.z));
+}
+
+__host__ __device__ constexpr bool alg_skips_free(int a) {
+    return a == PPT_ALG_LEAPFROG || a == PPT_ALG_BORIS || a == PPT_ALG_BORIS_REL;
+}
+
+// Steps a particle moving at v certainly stays outside every map, so that
+// they are field-free drift steps (only for fields without constant parts):
+// outside the union box of the maps on some axis, it must travel `dist` at
+// `rate` per step to come back on that axis.  After j steps the position
+// carries at most j * 2^-53 * X of rounding (X bounds |x| on the way), which
+// the margin covers.
+__device__ __forceinline__ int quiet_steps_f64(const FieldsDev& F, V3 r, V3 v, double dt) {
+    if (F.n_maps == 0) return 0;
+    const double x[3] = {r.x, r.y, r.z}, u[3] = {v.x * dt, v.y * dt, v.z * dt};
+    double best = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        double dist, rate, bound;
+        if (x[a] < F.box_lo[a]) {
+            dist = F.box_lo[a] - x[a];
+            rate = u[a];
+            bound = F.box_lo[a];
+        } else if (x[a] > F.box_hi[a]) {
+            dist = x[a] - F.box_hi[a];
+            rate = -u[a];
+            bound = F.box_hi[a];
+        } else {
+            continue;
+        }
+        const double X = fmax(fabs(x[a]), fabs(bound));
+        const double k = rate > 0.0 ? dist / (rate + 2.3e-16 * X) : 2e9;
+        best = fmax(best, k);
+    }
+    best = best * (1.0 - 1e-9) - 2.0;
+    return best <= 0.0 ? 0 : (best >= 1e9 ? 1000000000 : (int)best);
+}
+
+// One step; returns true for a field-free step of the Boris family (its
+// velocity update skipped, see below).
 template <int ALG, bool RF>
-__device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, int64_t g) {
+__device__ __forceinline__ bool step(Ctx& c, V3& r, V3& w, int64_t g) {
     const double dt = c.dt, qm = c.qm;
     if constexpr (ALG == PPT_ALG_RK4 || ALG == PPT_ALG_RK4_REL) {
         constexpr bool REL = ALG == PPT_ALG_RK4_REL;
@@ -201,21 +244,23 @@ __device__ __forceinline__ void step(Ctx& c, V3& r, V3& w, int64_t g) {
         const bool any = fields_at<RF>(c, r, g, 0.0, E, B) != 0 || c.const_nz;
         if constexpr (ALG == PPT_ALG_LEAPFROG) {
             if (any) w = w + lorentz(w, E, B, qm) * dt;
-            r = r + w * dt;
+            r = drift(r, w, dt);
         } else if constexpr (ALG == PPT_ALG_BORIS) {
             if (any) w = boris_v(w, E, B, dt, qm);
-            r = r + w * dt;
+            r = drift(r, w, dt);
         } else if constexpr (ALG == PPT_ALG_VAY_REL) {
             w = vay_rel_v(w, E, B, dt, qm);
-            r = r + w * dt;
+            r = drift(r, w, dt);
         } else if constexpr (ALG == PPT_ALG_BORIS_REL) {
             if (any) w = boris_rel_u(w, E, B, dt, qm);
-            r = r + w_to_v<ALG>(w) * dt;
+            r = drift(r, w_to_v<ALG>(w), dt);
         } else {  // PPT_ALG_VAY
             w = vay_u(w, E, B, dt, qm);
-            r = r + w_to_v<ALG>(w) * dt;
+            r = drift(r, w_to_v<ALG>(w), dt);
         }
+        return alg_skips_free(ALG) && !any;
     }
+    return false;
 }
 
 __device__ __forceinline__ void write_row(double* hist, int64_t rec, int64_t n, int64_t row, V3 a) {
@@ -271,11 +316,29 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
         // record-free segments: the inner loop carries only its counter
         int k = 0;
+        int quiet = 0;   // upcoming steps known to be field-free (quiet_steps_f64)
         while (k < nsteps) {
             const int64_t to_rec = (int64_t)until + 1;
             const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
             const int64_t g0 = P.step0 + k;
-            for (int i = 0; i < seg; ++i) step<ALG, RF>(c, r, w, g0 + i);
+            if constexpr (alg_skips_free(ALG)) {
+                for (int i = 0; i < seg;) {
+                    if (quiet > 0) {
+                        // a run of field-free steps: the same position advance, no field lookups
+                        const int m = quiet < seg - i ? quiet : seg - i;
+                        const V3 v = w_to_v<ALG>(w);
+#pragma unroll 1
+                        for (int j = 0; j < m; ++j) r = drift(r, v, P.dt);
+                        i += m;
+                        quiet -= m;
+                    } else {
+                        if (step<ALG, RF>(c, r, w, g0 + i)) quiet = quiet_steps_f64(P.F, r, w_to_v<ALG>(w), P.dt);
+                        ++i;
+                    }
+                }
+            } else {
+                for (int i = 0; i < seg; ++i) step<ALG, RF>(c, r, w, g0 + i);
+            }
             k += seg;
             if ((int64_t)seg == to_rec) {
                 const int64_t rec = (P.step0 + k) / P.rec_every;
@@ -311,7 +374,7 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
 }
 
 template <int ALG, bool RF>
-__global__ void __launch_bounds__(128) track_f64_kernel(const __grid_constant__ TrackDev P) {
+__global__ void __launch_bounds__(128, alg_skips_free(ALG) ? 5 : 1) track_f64_kernel(const __grid_constant__ TrackDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
     Ctx c = make_ctx(P);

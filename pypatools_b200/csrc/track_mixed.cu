@@ -133,9 +133,10 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
             double ph = fma((double)g, c.P->wdt, c.phase);
             if (toff != 0.0) ph = fma(c.P->omega, toff, ph);
             double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
-            // the argument is already in [-pi, pi], where the hardware cosine's
-            // absolute error (2^-21.4) is below the float32 field values' own
-            float cf = __cosf((float)red);
+            // the argument is already in [-pi, pi], so cosf takes its short
+            // path; the hardware __cosf (absolute error 2^-21.4, six times the
+            // float32 rounding of the field values) doubled the error tail
+            float cf = cosf((float)red);
             E = cf * E;
         }
     }
@@ -251,13 +252,75 @@ struct Drift {
     bool inside;
 };
 
+// Field-free step of the Boris family: the position advance by the high
+// part of the increment (the low part, a 3e-8 relative correction of the
+// displacement, is left out) and a branch-free carry of whole cells.
+__device__ __forceinline__ void drift_one(float cf[3], float f[3], const float dh[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float x = f[a] + dh[a];
+        const float cc = floorf(x);
+        f[a] = x - cc;
+        cf[a] += cc;
+    }
+}
+
+// m field-free steps in a row: four position advances per whole-cell carry
+// (in between, the offset stays below 1 + 4 |dh| cells).
+__device__ __forceinline__ void drift_steps(float cf[3], float f[3], const float dh[3], int m) {
+    int j = 0;
+    for (; j + 4 <= m; j += 4) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            float x = f[a] + dh[a];
+            x = x + dh[a];
+            x = x + dh[a];
+            x = x + dh[a];
+            const float cc = floorf(x);
+            f[a] = x - cc;
+            cf[a] += cc;
+        }
+    }
+    for (; j < m; ++j) drift_one(cf, f, dh);
+}
+
+// Steps the particle certainly stays outside the cell range of the map (the
+// pre-test of family_step), so that they are field-free drift steps: it is
+// outside on some axis and must travel `dist` cells at `rate` cells per step
+// to come back on that axis.  Each drift step moves the offset with a rounding
+// error below 2^-24 (5 |dh| + 2) cells (the offset is below 1 + 4 |dh| between
+// carries); that and the rounding of this estimate are covered by the margin,
+// so every step counted here is one the pre-test would have sent down the
+// drift branch.
+__device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cf[3], const float f[3],
+                                           const float dh[3]) {
+    float best = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float dist, rate;
+        if (cf[a] < 0.0f) {
+            dist = -cf[a] - f[a];                          // back in range once cf + f >= 0
+            rate = dh[a];
+        } else if (cf[a] > P.cell_max[a]) {
+            dist = (cf[a] - (P.cell_max[a] + 1.0f)) + f[a];   // back once cf + f < cell_max + 1
+            rate = -dh[a];
+        } else {
+            continue;
+        }
+        const float k = rate > 0.0f ? dist / (rate + 1.2e-7f * fmaf(5.0f, fabsf(dh[a]), 2.0f)) : 2e9f;
+        best = fmaxf(best, k);
+    }
+    best = fmaf(best, 0.99999f, -2.0f);
+    return best <= 0.0f ? 0 : (best >= 1e9f ? 1000000000 : (int)best);
+}
+
 // One step of the Boris family (Boris, leapfrog) with float-valued cell
 // indices (exact integers below 2^24).  Outside the map with no constant
 // field both updates leave v exactly unchanged (every added term is zero), so
-// such a step is only the position advance: two adds of the float-float
-// increment and a branch-free carry of whole cells.
+// such a step is only the position advance.  Returns true for such a
+// field-free step.
 template <int ALG, bool RF>
-__device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
+__device__ __forceinline__ bool family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
                                             int64_t g) {
     const TrackMixDev& P = *c.P;
     // cheap pre-test on the cell range (the last node layer included); the
@@ -281,17 +344,10 @@ __device__ __forceinline__ void family_step(MixCtx& c, float cf[3], float f[3], 
             f[a] = x - cc;   // in [0, 1]: 1 only for x a hair below an integer, the same point as (cc + 1, 0)
             cf[a] += cc;
         }
-        return;
+        return false;
     }
-    // Drift: no field acts, so the low part of the increment (a 3e-8 relative
-    // correction of the displacement) is left out.
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float x = f[a] + d.dh[a];
-        const float cc = floorf(x);
-        f[a] = x - cc;
-        cf[a] += cc;
-    }
+    drift_one(cf, f, d.dh);
+    return true;
 }
 
 template <int ALG, bool RF>
@@ -398,11 +454,22 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             float cf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
             // record-free segments: the inner loop carries only its counter
             int k = 0;
+            int quiet = 0;   // upcoming steps known to be field-free (quiet_steps)
             while (k < nsteps) {
                 const int64_t to_rec = (int64_t)until + 1;
                 const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
                 const int64_t g0 = P.step0 + k;
-                for (int i = 0; i < seg; ++i) family_step<ALG, RF>(c, cf, f, vh, vl, d, g0 + i);
+                for (int i = 0; i < seg;) {
+                    if (quiet > 0) {
+                        const int m = quiet < seg - i ? quiet : seg - i;
+                        drift_steps(cf, f, d.dh, m);
+                        i += m;
+                        quiet -= m;
+                    } else {
+                        if (family_step<ALG, RF>(c, cf, f, vh, vl, d, g0 + i)) quiet = quiet_steps(P, cf, f, d.dh);
+                        ++i;
+                    }
+                }
                 k += seg;
                 if ((int64_t)seg == to_rec) {
                     const int64_t rec = (P.step0 + k) / P.rec_every;

@@ -249,7 +249,8 @@ class TrackingServer:
             # 1) enqueue this tick for the current job set
             ticked = False
             if self.active:
-                if self.use_graphs and self._graph is None and stable >= 1:
+                # capture only with no result copy in flight: a capture forbids pageable copies in any thread
+                if self.use_graphs and self._graph is None and stable >= 1 and not collecting:
                     self._capture()
                 ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 ev0.record(self.compute)
@@ -261,7 +262,8 @@ class TrackingServer:
             # 2) while it runs: results of jobs finished last tick, then arrivals
             collecting += [(job, self._collect(job, t_start - clock_offset)) for job in retiring]
             retiring = []
-            collecting = self._finish(collecting, finished, block=not self.active and not pending)
+            # with nothing to run, wait for the copies: they free the memory the next arrivals need
+            collecting = self._finish(collecting, finished, block=not self.active and not joining)
             t2 = time.perf_counter()
             host["collect"] += t2 - t1
             now = t2 - t_start + clock_offset
@@ -271,7 +273,7 @@ class TrackingServer:
             while pending and pending[0].arrival <= now:
                 job = pending[0]
                 if self.used_bytes + job.device_bytes() > self.budget:
-                    if not self.active and not joining:
+                    if not self.active and not joining and not collecting:
                         raise MemoryError(f"job {job.job_id} needs {job.device_bytes()} B, budget {self.budget}")
                     break
                 pending.popleft()

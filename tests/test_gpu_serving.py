@@ -63,3 +63,16 @@ def test_serving_budget_queues_jobs(cuda):
     assert rep["jobs"] == len(jobs)
     assert server.used_bytes == 0
     _check_alone(ion, jobs)
+
+
+def test_serving_realtime_stream_with_graphs(cuda):
+    # jobs keep arriving while earlier ones retire: result copies run on the
+    # worker thread while later ticks are captured and replayed
+    fields = _map_fields()
+    ion, jobs = _jobs(fields, n_jobs=24, spacing=0.004)
+    server = TrackingServer(chunk=16, use_graphs=True)
+    rep = server.run(jobs, realtime=True)
+    assert rep["jobs"] == len(jobs)
+    assert server.used_bytes == 0
+    assert rep["p99_latency_s"] is not None and rep["p99_latency_s"] >= rep["p50_latency_s"] > 0
+    _check_alone(ion, jobs)
