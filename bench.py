@@ -287,6 +287,24 @@ def main():
                "against": "float64 GPU form (pinned to the oracle at 1e-10)"}
         del r_fp64, v_fp64
 
+    # time per phase of the job from the per-launch events: the bunch crosses
+    # the map during the first steps (each proton exits after 225-1225 steps,
+    # the in-map steps are 3.6 % of the job); the rest is field-free drift
+    in_map_steps = 1300
+
+    def phase_ms(res):
+        per_job = len(res["launch_ms"]) // max(1, args.steps)
+        first = [ms for i, ms in enumerate(res["launch_ms"]) if (i % per_job) * chunk < in_map_steps]
+        return sum(first) / args.steps, (sum(res["launch_ms"]) - sum(first)) / args.steps
+
+    phases = {"split_at_step": in_map_steps}
+    for form, res in results.items():
+        a, b = phase_ms(res)
+        phases[form] = {"ms_map_crossing": a, "ms_drift": b}
+    if "fp64" in results:
+        phases["mixed_over_fp64_map_crossing"] = phases["fp64"]["ms_map_crossing"] / phases["mixed"]["ms_map_crossing"]
+        phases["mixed_over_fp64_drift"] = phases["fp64"]["ms_drift"] / phases["mixed"]["ms_drift"]
+
     total_ps = n * wl.nsteps * args.steps * world
     m = results["mixed"]
     value = total_ps / (m["ms_total"] / 1e3)
@@ -363,6 +381,7 @@ def main():
             "fp64": ({"value": total_ps / (f64["ms_total"] / 1e3), "ms_per_step": f64["ms_per_job"],
                       "launches": f64["launches"]} if f64 else None),
             "mixed_over_fp64": (f64["ms_total"] / m["ms_total"]) if f64 else None,
+            "phases": phases,
             "error_vs_fp64": err,
             "roofline": roofline,
             "cpu_baseline": cpu,
