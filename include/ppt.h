@@ -131,6 +131,9 @@ int ppt_field_eval(const ppt_fields* fields, int64_t n, const double* pts,
  *   PPT_PREC_F64:   f64[6*n]  = x | y | z | w_x | w_y | w_z
  *   PPT_PREC_MIXED: i32[3*n]  = cell i | j | k  (on map 0's grid)
  *                   f32[9*n]  = offset x|y|z | w_hi x|y|z | w_lo x|y|z
+ *                   (position = lo + (cell + offset) d; the offset is in [0, 1]
+ *                   after steps that may see a field and may pass 1 between
+ *                   the whole-cell carries of field-free steps)
  * w is the velocity v [m/s], or u = gamma v for BORIS_REL / VAY. */
 typedef struct {
     int32_t precision;
@@ -215,8 +218,11 @@ int ppt_jobs_progress(const ppt_jobs* jobs, int64_t** steps, int32_t** done);
 
 int ppt_jobs_destroy(ppt_jobs* jobs);
 
-/* Reorder particles by cell (locality of the corner gathers).  Permutes the
- * state, rf_phase and order arrays in place.  Needs n_cells_hint >= 1.
+/* Reorder particles by the cell of map 0 (locality of the corner gathers).
+ * Permutes the state, rf_phase and order arrays in place.  Decided on the
+ * device: the permutation runs when at least n/16 particles are inside the
+ * map, or when the warps holding in-map particles exceed the ones they need
+ * by n/512; otherwise the call is a no-op that never waits on the host.
  * scratch: device buffer of ppt_cell_sort_scratch_bytes(n) bytes. */
 int64_t ppt_cell_sort_scratch_bytes(int64_t n);
 int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* order, double* rf_phase,

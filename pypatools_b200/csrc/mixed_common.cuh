@@ -1,9 +1,12 @@
 // Helpers for the mixed-precision form.
 //
-// Position: an int32 cell index per axis plus a float32 offset in [0, 1) in
-// cell units on the map's uniform grid, so x = lo + (cell + offset) d.  The
-// offset IS the trilinear weight of the reference's interpolation
-// (interpolators.py:109-115), so no floor or division happens per step.
+// Position: an int32 cell index per axis plus a float32 offset in cell units
+// on the map's uniform grid, so x = lo + (cell + offset) d.  After a step
+// that may see a field the offset is in [0, 1] and IS the trilinear weight of
+// the reference's interpolation (interpolators.py:109-115), so no floor or
+// division happens per step; field-free Boris-family steps carry whole cells
+// only every fourth global step, so between those the offset may run past 1
+// (the represented position is exact either way).
 // Velocity: an unevaluated float32 pair (hi + lo).  Per-step increments are
 // computed in float32 and added with an error-free two-sum, so rounding does
 // not random-walk the state at float32 precision.

@@ -6,10 +6,13 @@
 // (k fastest) modulo 2^22 -- exact for maps up to 4M cells, a hash beyond;
 // particles outside the map share one last bucket.  Histogram -> exclusive
 // scan -> scatter into a scratch copy -> copy back, with warp-aggregated
-// atomics (lanes with equal keys combine before touching memory).  When
-// fewer than 1/16 of the particles are inside the map the reordering buys
-// nothing, and every kernel after the histogram returns at once: the sort is
-// a no-op decided on the device, so the caller's stream never waits.
+// atomics (lanes with equal keys combine before touching memory).  The
+// reordering runs when at least 1/16 of the particles are inside the map, or
+// when the warps holding in-map particles exceed the ones those particles
+// need by n/512 (a few particles still in the map after the bunch has left,
+// spread over many warps: each such warp runs the gather path for one lane).
+// Otherwise every kernel after the histogram returns at once: the sort is a
+// no-op decided on the device, so the caller's stream never waits.
 // Order inside a bucket is arbitrary; `order` records slot -> row so outputs
 // land in the caller's row order, and each particle's arithmetic is
 // independent of its slot.
@@ -41,14 +44,17 @@ __device__ __forceinline__ uint32_t bucket_of_cells(const SortGeom& G, int c0, i
     return (uint32_t)(lin % G.n_in);
 }
 
-// Histogram of the in-map keys (one atomic per distinct key per warp) and the
-// in-map count (one atomic per block).  Particles outside the map touch no
-// counter: their bucket's size is n minus the in-map count, filled in by the
-// scan, so a bunch that has left the map costs no same-address atomics.
+// Histogram of the in-map keys (one atomic per distinct key per warp), the
+// in-map count and the number of warps with an in-map particle (one atomic
+// each per block).  Particles outside the map touch no counter: their
+// bucket's size is n minus the in-map count, filled in by the scan, so a
+// bunch that has left the map costs no same-address atomics.  Called by every
+// thread of the block (full warps).
 __device__ __forceinline__ void count_key(uint32_t b, bool inside, uint32_t* count, uint32_t* ctrl) {
-    __shared__ unsigned block_in;
-    if (threadIdx.x == 0) block_in = 0;
+    __shared__ unsigned block_in, block_warps;
+    if (threadIdx.x == 0) block_in = block_warps = 0;
     __syncthreads();
+    if (__any_sync(0xffffffffu, inside) && (threadIdx.x & 31) == 0) atomicAdd(&block_warps, 1u);
     if (inside) {
         const unsigned active = __activemask();
         const unsigned same = __match_any_sync(active, b);
@@ -59,7 +65,10 @@ __device__ __forceinline__ void count_key(uint32_t b, bool inside, uint32_t* cou
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && block_in) atomicAdd(ctrl, block_in);
+    if (threadIdx.x == 0 && block_in) {
+        atomicAdd(ctrl, block_in);
+        atomicAdd(ctrl + 1, block_warps);
+    }
 }
 
 __global__ void sort_keys_f64(int64_t n, const double* __restrict__ st, SortGeom G, uint32_t* __restrict__ key,
@@ -90,7 +99,8 @@ __global__ void sort_keys_mixed(int64_t n, const int32_t* __restrict__ ci, SortG
 }
 
 __device__ __forceinline__ bool sort_wanted(const uint32_t* ctrl, int64_t n) {
-    return (int64_t)ctrl[0] * 16 >= n;
+    const int64_t in = ctrl[0], excess_warps = (int64_t)ctrl[1] - (in + 31) / 32;
+    return in * 16 >= n || (in > 0 && excess_warps * 512 >= n);
 }
 
 __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* sh, uint32_t& total) {
@@ -271,7 +281,7 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
     const int block = 256;
 
     PPT_CUDA_TRY(cudaMemsetAsync(count, 0, (size_t)nb * 4, s));
-    PPT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, 4, s));
+    PPT_CUDA_TRY(cudaMemsetAsync(ctrl, 0, 8, s));
     if (st->precision == PPT_PREC_F64)
         sort_keys_f64<<<grid_for(n, block), block, 0, s>>>(n, st->f64, G, key, count, ctrl);
     else

@@ -270,19 +270,6 @@ __device__ __forceinline__ void write_row(double* hist, int64_t rec, int64_t n, 
     p[2] = a.z;
 }
 
-__device__ __forceinline__ void add_counters(unsigned long long* counters, unsigned hits, unsigned steps) {
-    unsigned long long h = hits, s = steps;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        h += __shfl_down_sync(0xffffffffu, h, o);
-        s += __shfl_down_sync(0xffffffffu, s, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(counters, h);
-        atomicAdd(counters + 1, s);
-    }
-}
-
 __device__ __forceinline__ Ctx make_ctx(const TrackDev& P) {
     return Ctx{&P.F, P.dt, P.qm, P.omega, 0.0, P.t0, 0u, P.F.e_const_nz | P.F.b_const_nz};
 }
@@ -379,7 +366,7 @@ __global__ void __launch_bounds__(128, alg_skips_free(ALG) ? 5 : 1) track_f64_ke
     unsigned steps_done = 0;
     Ctx c = make_ctx(P);
     if (s < P.n) steps_done = track_f64_particle<ALG, RF>(P, s, c);
-    if (P.counters) add_counters(P.counters, c.hits, steps_done);
+    if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
 }
 
 // Serving: a persistent block-level work queue over the float64 jobs of one
@@ -419,7 +406,7 @@ __global__ void __launch_bounds__(kJobBlock) track_f64_jobs_kernel(const __grid_
             Ctx c = make_ctx(sP);
             unsigned sd = 0;
             if (s < sP.n) sd = track_f64_particle<ALG, RF>(sP, s, c);
-            if (sP.counters) add_counters(sP.counters, c.hits, sd);
+            if (sP.counters) block_add_counters(sP.counters, c.hits, sd);
         }
         __syncthreads();
     }

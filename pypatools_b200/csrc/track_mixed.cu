@@ -44,14 +44,6 @@ __device__ __forceinline__ float tri8(Get get, float tx, float ty, float tz) {
     return lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
 }
 
-// In-domain test of a cell + offset position (the reference's bounds test).
-__device__ __forceinline__ bool mixed_inside(const TrackMixDev& P, const int cell[3], const float f[3]) {
-    int i;
-    float t;
-    return mixed_axis(cell[0], f[0], P.G.n[0], i, t) && mixed_axis(cell[1], f[1], P.G.n[1], i, t) &&
-           mixed_axis(cell[2], f[2], P.G.n[2], i, t);
-}
-
 // Trilinear E/B at (cell, offset) from the float32 map; returns false when
 // outside (fields = the constant parts only).
 __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3], F3& E,
@@ -245,64 +237,72 @@ __device__ __forceinline__ void increment(const TrackMixDev& P, const float vh[3
     }
 }
 
-// Per-particle loop state of the Boris family: increment and in-map flag.
+// Per-particle loop state of the Boris family: the position increment.
 struct Drift {
     float dh[3];
     float dl[3];
-    bool inside;
 };
 
-// Field-free step of the Boris family: the position advance by the high
-// part of the increment (the low part, a 3e-8 relative correction of the
-// displacement, is left out) and a branch-free carry of whole cells.
-__device__ __forceinline__ void drift_one(float cf[3], float f[3], const float dh[3]) {
+// Field-free steps of the Boris family (Boris, leapfrog).  Outside the map
+// with no constant field both updates leave v exactly unchanged (every added
+// term is zero), so such a step is the position advance by the high part of
+// the increment alone (the low part is a 3e-8 relative correction of the
+// displacement).  The whole-cell carry is taken after global steps g with
+// (g + 1) % 4 == 0 only; in between the offset runs up to 1 + 4 |dh| cells.
+// Because the carry points depend on the global step index alone, a track
+// gives the same bits however its steps are split into launches, runs or
+// serving ticks.  Normalising (cf + floor f, f - floor f) is exact, so the
+// represented position never depends on it.
+__device__ __forceinline__ void carry(float cf[3], float f[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float x = f[a] + dh[a];
-        const float cc = floorf(x);
-        f[a] = x - cc;
+        const float cc = floorf(f[a]);
+        f[a] -= cc;
         cf[a] += cc;
     }
 }
 
-// m field-free steps in a row: four position advances per whole-cell carry
-// (in between, the offset stays below 1 + 4 |dh| cells).
-__device__ __forceinline__ void drift_steps(float cf[3], float f[3], const float dh[3], int m) {
-    int j = 0;
-    for (; j + 4 <= m; j += 4) {
+__device__ __forceinline__ void add_dh(float f[3], const float dh[3]) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float x = f[a] + dh[a];
-            x = x + dh[a];
-            x = x + dh[a];
-            x = x + dh[a];
-            const float cc = floorf(x);
-            f[a] = x - cc;
-            cf[a] += cc;
-        }
+    for (int a = 0; a < 3; ++a) f[a] += dh[a];
+}
+
+// m field-free steps from global step g0.
+__device__ __forceinline__ void drift_steps(float cf[3], float f[3], const float dh[3], int64_t g0, int m) {
+    int j = 0;
+    for (; j < m && ((unsigned)(g0 + j) & 3u) != 0u; ++j) {
+        add_dh(f, dh);
+        if (((unsigned)(g0 + j + 1) & 3u) == 0u) carry(cf, f);
     }
-    for (; j < m; ++j) drift_one(cf, f, dh);
+    for (; j + 4 <= m; j += 4) {
+        add_dh(f, dh);
+        add_dh(f, dh);
+        add_dh(f, dh);
+        add_dh(f, dh);
+        carry(cf, f);
+    }
+    for (; j < m; ++j) add_dh(f, dh);   // fewer than 4 steps from an aligned start: no carry point
 }
 
 // Steps the particle certainly stays outside the cell range of the map (the
 // pre-test of family_step), so that they are field-free drift steps: it is
 // outside on some axis and must travel `dist` cells at `rate` cells per step
-// to come back on that axis.  Each drift step moves the offset with a rounding
-// error below 2^-24 (5 |dh| + 2) cells (the offset is below 1 + 4 |dh| between
-// carries); that and the rounding of this estimate are covered by the margin,
-// so every step counted here is one the pre-test would have sent down the
-// drift branch.
-__device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cf[3], const float f[3],
+// to come back on that axis.  (cn, fn) is the normalised position.  Each drift
+// step moves the offset with a rounding error below 2^-24 (5 |dh| + 2) cells
+// (the offset stays below 1 + 4 |dh| between carries); that and the rounding
+// of this estimate are covered by the margin, so every step counted here is
+// one the pre-test would have sent down the drift branch.
+__device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cn[3], const float fn[3],
                                            const float dh[3]) {
     float best = 0.0f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         float dist, rate;
-        if (cf[a] < 0.0f) {
-            dist = -cf[a] - f[a];                          // back in range once cf + f >= 0
+        if (cn[a] < 0.0f) {
+            dist = -cn[a] - fn[a];                          // back in range once cn + fn >= 0
             rate = dh[a];
-        } else if (cf[a] > P.cell_max[a]) {
-            dist = (cf[a] - (P.cell_max[a] + 1.0f)) + f[a];   // back once cf + f < cell_max + 1
+        } else if (cn[a] > P.cell_max[a]) {
+            dist = (cn[a] - (P.cell_max[a] + 1.0f)) + fn[a];   // back once cn + fn < cell_max + 1
             rate = -dh[a];
         } else {
             continue;
@@ -314,40 +314,48 @@ __device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cf[
     return best <= 0.0f ? 0 : (best >= 1e9f ? 1000000000 : (int)best);
 }
 
-// One step of the Boris family (Boris, leapfrog) with float-valued cell
-// indices (exact integers below 2^24).  Outside the map with no constant
-// field both updates leave v exactly unchanged (every added term is zero), so
-// such a step is only the position advance.  Returns true for such a
-// field-free step.
+// One step g of the Boris family with float-valued cell indices (exact
+// integers below 2^24).  Returns the number of following steps known to be
+// field-free (0 when this step met a field or the particle may come back).
 template <int ALG, bool RF>
-__device__ __forceinline__ bool family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
-                                            int64_t g) {
+__device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
+                                           int64_t g) {
     const TrackMixDev& P = *c.P;
+    float cn[3], fn[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float cc = floorf(f[a]);
+        cn[a] = cf[a] + cc;
+        fn[a] = f[a] - cc;
+    }
     // cheap pre-test on the cell range (the last node layer included); the
     // exact bounds rule is applied inside gather_mixed
-    const bool maybe = (cf[0] >= 0.0f) & (cf[0] <= P.cell_max[0]) & (cf[1] >= 0.0f) & (cf[1] <= P.cell_max[1]) &
-                       (cf[2] >= 0.0f) & (cf[2] <= P.cell_max[2]);
+    const bool maybe = (cn[0] >= 0.0f) & (cn[0] <= P.cell_max[0]) & (cn[1] >= 0.0f) & (cn[1] <= P.cell_max[1]) &
+                       (cn[2] >= 0.0f) & (cn[2] <= P.cell_max[2]);
     if (maybe || P.const_nz) {
-        const int cell[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
+        const int cell[3] = {(int)cn[0], (int)cn[1], (int)cn[2]};
         F3 E, B;
-        if (fields_mixed<RF>(c, cell, f, g, 0.0, E, B)) {
+        if (fields_mixed<RF>(c, cell, fn, g, 0.0, E, B)) {
             F3 v = f3(vh[0], vh[1], vh[2]);
             vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
             increment(P, vh, vl, d.dh, d.dl);
         }
-        // where fields act, the full float-float increment
+        // where fields act (or may), the full float-float increment and a carry
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            float x = f[a] + d.dh[a];
+            float x = fn[a] + d.dh[a];
             x = x + d.dl[a];
             const float cc = floorf(x);
             f[a] = x - cc;   // in [0, 1]: 1 only for x a hair below an integer, the same point as (cc + 1, 0)
-            cf[a] += cc;
+            cf[a] = cn[a] + cc;
         }
-        return false;
+        return 0;
     }
-    drift_one(cf, f, d.dh);
-    return true;
+    add_dh(f, d.dh);
+    if (((unsigned)(g + 1) & 3u) == 0u) carry(cf, f);
+    // the next steps' pre-test, decided now from the normalised position
+    add_dh(fn, d.dh);
+    return quiet_steps(P, cn, fn, d.dh);
 }
 
 template <int ALG, bool RF>
@@ -445,7 +453,6 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
         }
         Drift d;
         increment(P, vh, vl, d.dh, d.dl);
-        d.inside = mixed_inside(P, cell, f);
         const int nsteps = (int)P.nsteps;
         const int rec_every = P.rec_every > 0x7fffffff ? 0x7fffffff : (int)P.rec_every;
         const int64_t until64 = P.rec_every - 1 - (P.step0 % P.rec_every);
@@ -462,11 +469,11 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 for (int i = 0; i < seg;) {
                     if (quiet > 0) {
                         const int m = quiet < seg - i ? quiet : seg - i;
-                        drift_steps(cf, f, d.dh, m);
+                        drift_steps(cf, f, d.dh, g0 + i, m);
                         i += m;
                         quiet -= m;
                     } else {
-                        if (family_step<ALG, RF>(c, cf, f, vh, vl, d, g0 + i)) quiet = quiet_steps(P, cf, f, d.dh);
+                        quiet = family_step<ALG, RF>(c, cf, f, vh, vl, d, g0 + i);
                         ++i;
                     }
                 }
@@ -480,6 +487,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                     until -= seg;
                 }
             }
+            // the state keeps its (possibly uncarried) offset; exact anyway
 #pragma unroll
             for (int a = 0; a < 3; ++a) cell[a] = (int)cf[a];
         } else {
@@ -497,7 +505,15 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
         if (P.flags & PPT_TRACK_FINAL) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
-                if (fields_mixed<RF>(c, cell, f, P.nsteps_total, 0.0, E, B))
+                int cn[3];
+                float fn[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {   // exact normalisation for the cell lookup
+                    const float cc = floorf(f[a]);
+                    cn[a] = cell[a] + (int)cc;
+                    fn[a] = f[a] - cc;
+                }
+                if (fields_mixed<RF>(c, cn, fn, P.nsteps_total, 0.0, E, B))
                     // Boris push with time step +dt/2 (pusher.py:993-1007)
                     vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt));
                 if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
@@ -520,26 +536,13 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
     return (unsigned)P.nsteps;
 }
 
-__device__ __forceinline__ void add_mixed_counters(unsigned long long* counters, unsigned hits, unsigned steps) {
-    unsigned long long h = hits, st = steps;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        h += __shfl_down_sync(0xffffffffu, h, o);
-        st += __shfl_down_sync(0xffffffffu, st, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(counters, h);
-        atomicAdd(counters + 1, st);
-    }
-}
-
 template <int ALG, bool RF>
 __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
     MixCtx c{&P, 0.0, 0u};
     if (s < P.n) steps_done = track_mixed_particle<ALG, RF>(P, s, c);
-    if (P.counters) add_mixed_counters(P.counters, c.hits, steps_done);
+    if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
 }
 
 // Serving: the mixed-precision counterpart of track_f64_jobs_kernel.
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
             MixCtx c{&sP, 0.0, 0u};
             unsigned sd = 0;
             if (s < sP.n) sd = track_mixed_particle<ALG, RF>(sP, s, c);
-            if (sP.counters) add_mixed_counters(sP.counters, c.hits, sd);
+            if (sP.counters) block_add_counters(sP.counters, c.hits, sd);
         }
         __syncthreads();
     }

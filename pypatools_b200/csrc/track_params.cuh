@@ -108,6 +108,35 @@ __device__ __forceinline__ void take_item(const JobQueueDev& Q, int* s_item, int
     __syncthreads();
 }
 
+// Add a block's in-map gathers and particle steps to the two device
+// counters: warp sums by shuffle, then one atomic pair per block (per-warp
+// atomics on the same two addresses serialised at the end of short launches).
+// Every thread of the block calls it.
+__device__ __forceinline__ void block_add_counters(unsigned long long* counters, unsigned hits, unsigned steps) {
+    __shared__ unsigned long long part[2][32];
+    unsigned long long h = hits, s = steps;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        h += __shfl_down_sync(0xffffffffu, h, o);
+        s += __shfl_down_sync(0xffffffffu, s, o);
+    }
+    const int warp = threadIdx.x >> 5, warps = (blockDim.x + 31) >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        part[0][warp] = h;
+        part[1][warp] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < warps; ++w) {
+            h += part[0][w];
+            s += part[1][w];
+        }
+        atomicAdd(counters, h);
+        atomicAdd(counters + 1, s);
+    }
+    __syncthreads();   // part[] is reused by the next call in the block
+}
+
 // Step window of a job in this tick: [step0, step0 + k) and its flags.
 __device__ __forceinline__ void job_window(const JobQueueDev& Q, int gjob, int64_t total, int64_t* step0,
                                            int64_t* k, int* flags) {

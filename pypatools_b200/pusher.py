@@ -172,6 +172,82 @@ class DeviceTracker:
             self.launches += 1
         self.step += k
 
+    def run(self, nsteps, chunk, sort_every=0, long_chunk=None, after_launch=None, launch_events=None,
+            stream=None, in_flight=2):
+        """Advance ``nsteps`` steps in launches of at most ``chunk`` steps.
+
+        With ``sort_every`` > 0 and maps present the schedule follows the
+        bunch: while the maps are populated, every launch of ``sort_every``
+        steps starts with a cell sort; once a finished launch spent less than
+        1/16 of its particle-steps inside a map, one more sort (it groups the
+        stragglers still inside, see ``ppt_cell_sort``) and then launches of
+        ``long_chunk`` steps without sorts, which read and write the state
+        less often; the sorted schedule returns when the in-map share rises
+        again.  The share comes from the device counters, copied to pinned
+        memory after each launch and read with a lag: at most ``in_flight``
+        launches are queued ahead, so the GPU never waits on the host.
+        ``after_launch(steps_done)`` runs after each launch is enqueued;
+        ``launch_events`` (a list) receives (start event, end event, first
+        step, steps) for each track launch."""
+        torch = self.torch
+        nsteps = int(nsteps)
+        chunk = max(1, int(chunk))
+        adaptive = sort_every > 0 and self.dfields.has_maps and self.n > 0
+        long_chunk = max(chunk, int(long_chunk or 10 * max(sort_every, 1)))
+        st = torch.cuda.current_stream(self.device) if stream is None else stream
+        if adaptive and self.counters is None:
+            self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
+        pending = []            # (event, pinned counters copy, steps in the launch)
+        last_hits = None
+        dense = True            # the maps hold a good share of the particles
+        sorted_sparse = False   # the grouping sort after the bunch left has been made
+        done = 0
+        if nsteps == 0:
+            self.advance(0, stream)
+            return
+        while done < nsteps:
+            if adaptive:
+                # newest in-map share from the launches that have finished
+                while pending and (len(pending) > in_flight or pending[0][0].query()):
+                    ev, host, k_done = pending.pop(0)
+                    ev.synchronize()
+                    hits = int(host[0])
+                    if last_hits is not None:
+                        frac = (hits - last_hits) / max(1, self.n * k_done)
+                        if frac * 16 >= 1:
+                            dense, sorted_sparse = True, False
+                        else:
+                            dense = False
+                    last_hits = hits
+                if dense or not sorted_sparse:
+                    if (self.step % sort_every == 0) or not dense:
+                        self.sort(stream)
+                    sorted_sparse = not dense
+                k = min(sort_every if dense else long_chunk, chunk if dense else long_chunk, nsteps - done)
+                if dense:
+                    k = min(k, sort_every - self.step % sort_every)
+            else:
+                k = min(chunk, nsteps - done)
+            if launch_events is not None:
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                step0 = self.step
+                a.record(st)
+                self.advance(k, stream)
+                b.record(st)
+                launch_events.append((a, b, step0, k))
+            else:
+                self.advance(k, stream)
+            done += k
+            if adaptive:
+                host = torch.empty(2, dtype=torch.int64, pin_memory=True)
+                with torch.cuda.stream(st):
+                    host.copy_(self.counters, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(st)
+                pending.append((ev, host, k))
+            if after_launch is not None:
+                after_launch(done)
+
     def sort(self, stream=None):
         """Reorder particles by cell (gather locality)."""
         torch = self.torch
@@ -349,21 +425,16 @@ class PusherGPU:
                         h_v[copied:upto].copy_(tr.v_hist[copied:upto], non_blocking=True)
                     copied = upto
             tr.load(self._upload(r0, df.device), self._upload(v0, df.device))
-            done = 0
-            if nsteps == 0:
-                tr.advance(0)
-            while done < nsteps:
-                if self.sort_every > 0 and done % self.sort_every == 0:
-                    tr.sort()
-                k = min(chunk, nsteps - done)
+
+            def after_launch(done):
                 if verbose:
                     print(f"Step {done}/{nsteps} ({100 * done / nsteps:.0f}%)")
-                tr.advance(k)
-                done += k
                 if to_host and done < nsteps:
                     # records 0 .. done // rec are final; the last one waits for
                     # the closing half step of the Boris family
                     drain(min(done // rec + 1, n_rec - 1))
+
+            tr.run(nsteps, chunk, sort_every=self.sort_every, after_launch=after_launch)
             if to_host:
                 drain(n_rec)
                 copy_stream.synchronize()

@@ -93,17 +93,23 @@ def test_trilinear_exact_on_linear_field(cuda):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_chunking_and_sorting_are_bitwise_invariant(cuda, precision):
-    wl = workloads.quad_solenoid_protons(n=3000, nsteps=300)
+@pytest.mark.parametrize("nsteps", [300, 1100])
+def test_chunking_and_sorting_are_bitwise_invariant(cuda, precision, nsteps):
+    # 1100 steps: the protons leave the map after about 360, so the field-free
+    # runs (and, in the mixed form, their whole-cell carries) are split by the
+    # launch boundaries differently in each schedule
+    wl = workloads.quad_solenoid_protons(n=3000, nsteps=nsteps)
     e, b = gpu_fields(wl)
-    base = PusherGPU(wl.species, "boris", precision=precision).track_batch(wl.r0, wl.v0, e, b, 300, wl.dt, 50)
+    base = PusherGPU(wl.species, "boris", precision=precision).track_batch(wl.r0, wl.v0, e, b, nsteps, wl.dt, 50)
     chunked = PusherGPU(wl.species, "boris", precision=precision, steps_per_launch=7).track_batch(
-        wl.r0, wl.v0, e, b, 300, wl.dt, 50)
+        wl.r0, wl.v0, e, b, nsteps, wl.dt, 50)
     sorted_ = PusherGPU(wl.species, "boris", precision=precision, sort_every=40).track_batch(
-        wl.r0, wl.v0, e, b, 300, wl.dt, 50)
+        wl.r0, wl.v0, e, b, nsteps, wl.dt, 50)
     for other in (chunked, sorted_):
         np.testing.assert_array_equal(base[0], other[0])
         np.testing.assert_array_equal(base[1], other[1])
+    if nsteps > 400:
+        assert np.all(np.abs(base[0][-1, :, 2]) > 0.05)   # every proton ended outside the map
 
 
 def test_nonfinite_input_warns(cuda):

@@ -20,9 +20,9 @@ def _map_fields(map_dtype=np.float32):
     return out
 
 
-def _jobs(fields, n_jobs=10, spacing=0.002):
+def _jobs(fields, n_jobs=10, spacing=0.002, steps_max=300):
     ion = IonSpecies("proton")
-    specs = workloads.serving_stream(n_jobs=n_jobs, n_min=200, n_max=3000, steps_min=40, steps_max=300,
+    specs = workloads.serving_stream(n_jobs=n_jobs, n_min=200, n_max=3000, steps_min=40, steps_max=steps_max,
                                      n_maps=len(fields))
     jobs = []
     for s in specs:
@@ -69,7 +69,9 @@ def test_serving_realtime_stream_with_graphs(cuda):
     # jobs keep arriving while earlier ones retire: result copies run on the
     # worker thread while later ticks are captured and replayed
     fields = _map_fields()
-    ion, jobs = _jobs(fields, n_jobs=24, spacing=0.004)
+    # up to 1500 steps: the bunches leave their maps, so field-free runs are
+    # split by the 16-step ticks here and by whole-track launches alone
+    ion, jobs = _jobs(fields, n_jobs=24, spacing=0.004, steps_max=1500)
     server = TrackingServer(chunk=16, use_graphs=True)
     rep = server.run(jobs, realtime=True)
     assert rep["jobs"] == len(jobs)
