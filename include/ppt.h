@@ -96,20 +96,48 @@ typedef struct {
 
 /* Create a zero-valued map on the current device.  has_e / has_b say which
  * fields it stores; store_dtype is PPT_DTYPE_F64 (plain form) or
- * PPT_DTYPE_F32 (mixed form, needs uniform axes). */
+ * PPT_DTYPE_F32 (mixed form, needs uniform axes).  The same as
+ * ppt_fieldmap_create_masked with the mask 0x07, 0x38 or 0x3F. */
 int ppt_fieldmap_create(const ppt_grid_desc* grid, int has_e, int has_b, int store_dtype,
                         ppt_fieldmap** out);
 
+/* Field components, bit c of a component mask (c = Ex, Ey, Ez, Bx, By, Bz). */
+#define PPT_COMP_EX 0x01
+#define PPT_COMP_EY 0x02
+#define PPT_COMP_EZ 0x04
+#define PPT_COMP_BX 0x08
+#define PPT_COMP_BY 0x10
+#define PPT_COMP_BZ 0x20
+
+/* Record layout a map storing the components of comp_mask uses: the
+ * smallest of the layouts {Bz}, {Ez Bz}, {Ex Ey Ez}, {Bx By Bz}, {Ex Ey Bz},
+ * {all six} that contains comp_mask, as a component mask.  Layouts of 1, 2
+ * or 3 components store them packed in Ex..Bz order in records of 1, 2 or
+ * 4 elements; the six-component layout is [Ex Ey Ez 0 | Bx By Bz 0].
+ * Returns PPT_ERR_ARG for a mask that is 0 or above 0x3F. */
+int ppt_fieldmap_layout(uint32_t comp_mask);
+
+/* Create a zero-valued map storing only the components of comp_mask (laid
+ * out as ppt_fieldmap_layout(comp_mask)): components that are identically
+ * zero in every term of a field need neither storage nor gathers, and the
+ * mixed-form kernels, compiled per layout, drop them from the arithmetic.
+ * The mixed form needs the six-component layout when the fields have
+ * constant parts (ppt_fields.e_const / b_const not zero). */
+int ppt_fieldmap_create_masked(const ppt_grid_desc* grid, uint32_t comp_mask, int store_dtype,
+                               ppt_fieldmap** out);
+
 /* map += scale[c] * comp[c] for c in (Ex,Ey,Ez,Bx,By,Bz).  comp[c] is a
  * DEVICE pointer to an n[0]*n[1]*n[2] C-contiguous array of src_dtype, or
- * NULL (adds nothing).  Used once per term of a composite / scaled field. */
+ * NULL (adds nothing); a component the map's layout does not store must be
+ * NULL.  Used once per term of a composite / scaled field. */
 int ppt_fieldmap_add(ppt_fieldmap* map, const void* const comp[6], const double scale[6],
                      int src_dtype, void* stream);
 
 int ppt_fieldmap_destroy(ppt_fieldmap* map);
 
 /* bytes of device memory held, and flags: bit0 has_e, bit1 has_b,
- * bit2 all axes uniform, bit3 float32 storage */
+ * bit2 all axes uniform, bit3 float32 storage, bits 8-13 the layout's
+ * component mask */
 int ppt_fieldmap_info(const ppt_fieldmap* map, int64_t* bytes, int* flags);
 
 /* The fields a pusher sees: E = e_const + sum over maps of the map's E,

@@ -5,7 +5,7 @@ importing the GPU entry points raises instead of falling back to the CPU.
 """
 import ctypes
 import os
-from ctypes import c_double, c_int, c_int32, c_int64, c_void_p, POINTER
+from ctypes import c_uint32, c_double, c_int, c_int32, c_int64, c_void_p, POINTER
 from pathlib import Path
 
 LIB_PATH = Path(os.environ.get("PPT_LIBRARY", Path(__file__).resolve().parent / "lib" / "libppt.so"))
@@ -21,6 +21,8 @@ DTYPE_F64, DTYPE_F32 = 0, 1
 TRACK_INIT, TRACK_FINAL = 1, 2
 STATUS_NONFINITE, STATUS_BOUNDS, STATUS_RANGE = 1, 2, 4
 MAX_MAPS = 4
+COMP_BITS = {"ex": 0x01, "ey": 0x02, "ez": 0x04, "bx": 0x08, "by": 0x10, "bz": 0x20}
+FULL_MASK = 0x3F
 MOMENTS_LEN = 22
 
 
@@ -67,6 +69,8 @@ class JobDesc(ctypes.Structure):
 # name -> (restype, argtypes); every symbol include/ppt.h declares
 SIGNATURES = {
     "ppt_fieldmap_create": (c_int, [POINTER(GridDesc), c_int, c_int, c_int, POINTER(c_void_p)]),
+    "ppt_fieldmap_layout": (c_int, [c_uint32]),
+    "ppt_fieldmap_create_masked": (c_int, [POINTER(GridDesc), c_uint32, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_add": (c_int, [c_void_p, POINTER(c_void_p * 6), POINTER(c_double * 6), c_int, c_void_p]),
     "ppt_fieldmap_destroy": (c_int, [c_void_p]),
     "ppt_fieldmap_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int)]),

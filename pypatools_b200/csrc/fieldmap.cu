@@ -1,5 +1,6 @@
 // Field maps: upload/accumulate of node values into the interleaved device
-// layout, and standalone E/B evaluation at arbitrary points.
+// layout (records storing only the components that are not identically
+// zero), and standalone E/B evaluation at arbitrary points.
 //
 // Reference behaviour restated here:
 //   Field.from_arrays builds one NumbaInterpolator per component on the
@@ -26,6 +27,24 @@ int pick_block(int64_t n) {
     if (n <= 148LL * 32) return 32;
     if (n <= 148LL * 64 * 2) return 64;
     return 128;
+}
+
+// Layout storing a component mask: the smallest compiled layout containing it.
+int layout_for(uint32_t comp_mask) {
+    if (comp_mask == 0 || comp_mask > 0x3F) return -1;
+    const int order[] = {kLayBz, kLayEzBz, kLayE, kLayB, kLayExEyBz, kLayFull};   // by size
+    for (int layout : order)
+        if ((comp_mask & ~(uint32_t)layout) == 0) return layout;
+    return kLayFull;
+}
+
+// Record slot of component c (0..5) in a layout, or -1 when not stored.
+int layout_slot(int layout, int c) {
+    if (!(layout & (1 << c))) return -1;
+    if (layout == kLayFull) return c < 3 ? c : c + 1;
+    int slot = 0;
+    for (int k = 0; k < c; ++k) slot += (layout >> k) & 1;
+    return slot;
 }
 
 // ---------------------------------------------------------------------------
@@ -90,26 +109,32 @@ __global__ void field_eval_kernel(const __grid_constant__ FieldsDev F, int64_t n
         Cell c;
         if (!locate(m, r, c)) continue;
         if (m.dtype == PPT_DTYPE_F64) {
-            if (m.has_e) E = E + gather_f64(m, c, 0);
-            if (m.has_b) B = B + gather_f64(m, c, m.b_off);
+            gather_map_f64(m, c, E, B);
         } else {
+            // float32 records: every stored slot, then by layout
             const float* base = static_cast<const float*>(m.data);
-            float tx = (float)c.tx, ty = (float)c.ty, tz = (float)c.tz;
-            for (int h = 0; h < 2; ++h) {
-                if (h == 0 && !m.has_e) continue;
-                if (h == 1 && !m.has_b) continue;
-                int off = h == 0 ? 0 : m.b_off;
-                float4 q[8];
-                for (int k = 0; k < 8; ++k) {
-                    int di = (k >> 2) & 1, dj = (k >> 1) & 1, dk = k & 1;
-                    int64_t node = c.base + di * m.sx + dj * m.sy + dk;
-                    q[k] = __ldg(reinterpret_cast<const float4*>(base + node * m.stride + off));
+            const float tx = (float)c.tx, ty = (float)c.ty, tz = (float)c.tz;
+            float val[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < m.stride; ++k) {
+                float q[8];
+                for (int corner = 0; corner < 8; ++corner) {
+                    const int di = (corner >> 2) & 1, dj = (corner >> 1) & 1, dk = corner & 1;
+                    const int64_t node = c.base + di * m.sx + dj * m.sy + dk;
+                    q[corner] = __ldg(base + node * m.stride + k);
                 }
-                V3 o = v3(tri_f(q[0].x, q[4].x, q[2].x, q[6].x, q[1].x, q[5].x, q[3].x, q[7].x, tx, ty, tz),
-                          tri_f(q[0].y, q[4].y, q[2].y, q[6].y, q[1].y, q[5].y, q[3].y, q[7].y, tx, ty, tz),
-                          tri_f(q[0].z, q[4].z, q[2].z, q[6].z, q[1].z, q[5].z, q[3].z, q[7].z, tx, ty, tz));
-                if (h == 0) E = E + o; else B = B + o;
+                val[k] = tri_f(q[0], q[4], q[2], q[6], q[1], q[5], q[3], q[7], tx, ty, tz);
             }
+            double comp[6];
+            for (int cc = 0; cc < 6; ++cc) {
+                int slot = -1;
+                if (m.layout & (1 << cc)) {
+                    if (m.layout == kLayFull) slot = cc < 3 ? cc : cc + 1;
+                    else { slot = 0; for (int k = 0; k < cc; ++k) slot += (m.layout >> k) & 1; }
+                }
+                comp[cc] = slot >= 0 ? (double)val[slot] : 0.0;
+            }
+            if (m.has_e) E = E + v3(comp[0], comp[1], comp[2]);
+            if (m.has_b) B = B + v3(comp[3], comp[4], comp[5]);
         }
     }
     if (e_out) { e_out[3 * p] = E.x; e_out[3 * p + 1] = E.y; e_out[3 * p + 2] = E.z; }
@@ -131,11 +156,27 @@ __device__ __forceinline__ float tri_f(float c000, float c100, float c010, float
 
 using namespace ppt;
 
+extern "C" int ppt_fieldmap_layout(uint32_t comp_mask) {
+    const int layout = layout_for(comp_mask);
+    if (layout < 0) return fail(PPT_ERR_ARG, "comp_mask must be in [1, 0x3F]");
+    return layout;
+}
+
 extern "C" int ppt_fieldmap_create(const ppt_grid_desc* grid, int has_e, int has_b, int store_dtype,
                                    ppt_fieldmap** out) {
+    if (!has_e && !has_b) {
+        if (out) *out = nullptr;
+        return fail(PPT_ERR_ARG, "a map must store E, B or both");
+    }
+    return ppt_fieldmap_create_masked(grid, (has_e ? 0x07u : 0u) | (has_b ? 0x38u : 0u), store_dtype, out);
+}
+
+extern "C" int ppt_fieldmap_create_masked(const ppt_grid_desc* grid, uint32_t comp_mask, int store_dtype,
+                                          ppt_fieldmap** out) {
     if (!grid || !out) return fail(PPT_ERR_ARG, "grid and out must not be NULL");
     *out = nullptr;
-    if (!has_e && !has_b) return fail(PPT_ERR_ARG, "a map must store E, B or both");
+    const int layout = layout_for(comp_mask);
+    if (layout < 0) return fail(PPT_ERR_ARG, "comp_mask must be in [1, 0x3F]");
     if (store_dtype != PPT_DTYPE_F64 && store_dtype != PPT_DTYPE_F32)
         return fail(PPT_ERR_ARG, "store_dtype must be PPT_DTYPE_F64 or PPT_DTYPE_F32");
     ppt_fieldmap m;
@@ -171,10 +212,11 @@ extern "C" int ppt_fieldmap_create(const ppt_grid_desc* grid, int has_e, int has
     m.dev.all_uniform = m.dev.ax[0].uniform && m.dev.ax[1].uniform && m.dev.ax[2].uniform;
     if (store_dtype == PPT_DTYPE_F32 && !m.dev.all_uniform)
         return fail(PPT_ERR_UNSUPPORTED, "float32 (mixed-precision) maps need uniform grid axes");
-    m.dev.has_e = has_e ? 1 : 0;
-    m.dev.has_b = has_b ? 1 : 0;
-    m.dev.stride = (has_e && has_b) ? 8 : 4;
-    m.dev.b_off = has_e ? 4 : 0;
+    m.dev.layout = layout;
+    m.dev.has_e = layout_has_e(layout) ? 1 : 0;
+    m.dev.has_b = layout_has_b(layout) ? 1 : 0;
+    m.dev.stride = layout_width(layout);
+    m.dev.b_off = layout == kLayFull ? 4 : 0;
     m.dev.dtype = store_dtype;
     m.dev.sy = m.n[2];
     m.dev.sx = m.n[1] * m.n[2];
@@ -219,10 +261,11 @@ extern "C" int ppt_fieldmap_add(ppt_fieldmap* map, const void* const comp[6], co
     const int grid = (int)(g > 148 * 32 ? 148 * 32 : g);
     for (int c = 0; c < 6; ++c) {
         if (!comp[c]) continue;
-        const bool is_e = c < 3;
-        if (is_e && !map->dev.has_e) return fail(PPT_ERR_ARG, "map does not store E");
-        if (!is_e && !map->dev.has_b) return fail(PPT_ERR_ARG, "map does not store B");
-        const int slot = (is_e ? 0 : map->dev.b_off) + (c % 3);
+        const int slot = layout_slot(map->dev.layout, c);
+        if (slot < 0) {
+            static const char* names[6] = {"Ex", "Ey", "Ez", "Bx", "By", "Bz"};
+            return fail(PPT_ERR_ARG, std::string("the map's layout does not store ") + names[c]);
+        }
         if (map->dev.dtype == PPT_DTYPE_F64) {
             double* dst = static_cast<double*>(map->data);
             if (src_dtype == PPT_DTYPE_F64)
@@ -264,7 +307,7 @@ extern "C" int ppt_fieldmap_info(const ppt_fieldmap* map, int64_t* bytes, int* f
     if (bytes) *bytes = (int64_t)map->bytes;
     if (flags)
         *flags = map->dev.has_e | (map->dev.has_b << 1) | (map->dev.all_uniform << 2) |
-                 ((map->dev.dtype == PPT_DTYPE_F32) << 3);
+                 ((map->dev.dtype == PPT_DTYPE_F32) << 3) | (map->dev.layout << 8);
     return PPT_OK;
 }
 

@@ -48,14 +48,31 @@ struct AxisDev {
     int uniform;
 };
 
+// Record layouts, named by the component mask they store (bit c = Ex, Ey,
+// Ez, Bx, By, Bz).  Up to three components are packed in Ex..Bz order in
+// records of 1, 2 or 4 elements; all six use [Ex Ey Ez 0 | Bx By Bz 0].
+constexpr int kLayFull = 0x3F;
+constexpr int kLayE = 0x07;
+constexpr int kLayB = 0x38;
+constexpr int kLayExEyBz = 0x23;
+constexpr int kLayEzBz = 0x24;
+constexpr int kLayBz = 0x20;
+
+__host__ __device__ constexpr int layout_width(int layout) {
+    return layout == kLayFull ? 8 : (layout == kLayEzBz ? 2 : (layout == kLayBz ? 1 : 4));
+}
+__host__ __device__ constexpr bool layout_has_e(int layout) { return (layout & 0x07) != 0; }
+__host__ __device__ constexpr bool layout_has_b(int layout) { return (layout & 0x38) != 0; }
+
 struct MapDev {
     const void* data;
     int64_t sx;       // node stride of i  (= ny*nz)
     int64_t sy;       // node stride of j  (= nz)
-    int stride;       // elements per node record (4 or 8)
+    int stride;       // elements per node record (1, 2, 4 or 8)
+    int layout;       // the kLay* component mask the records store
     int has_e;
     int has_b;
-    int b_off;        // element offset of B in the record (0 or 4)
+    int b_off;        // element offset of B in a full-layout record (4)
     int dtype;        // PPT_DTYPE_F64 / PPT_DTYPE_F32
     int all_uniform;
     AxisDev ax[3];
@@ -206,6 +223,64 @@ __device__ __forceinline__ V3 gather_f64(const MapDev& m, const Cell& c, int off
     return o;
 }
 
+__device__ __forceinline__ void ldg_f64x2(const double* p, double& a, double& b) {
+    asm volatile("ld.global.nc.v2.f64 {%0,%1}, [%2];" : "=d"(a), "=d"(b) : "l"(p));
+}
+
+// The K interpolated slots of a float64 map with 1- or 2-element records.
+template <int W>
+__device__ __forceinline__ void gather_slots_f64(const MapDev& m, const Cell& c, double out[W]) {
+    const double* base = static_cast<const double*>(m.data);
+    double v[8][W];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int di = (q >> 2) & 1, dj = (q >> 1) & 1, dk = q & 1;
+        const int64_t node = c.base + di * m.sx + dj * m.sy + dk;
+        if constexpr (W == 2) ldg_f64x2(base + node * 2, v[q][0], v[q][1]);
+        else v[q][0] = __ldg(base + node);
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        out[k] = tri(v[0][k], v[4][k], v[2][k], v[6][k], v[1][k], v[5][k], v[3][k], v[7][k], c.tx, c.ty, c.tz);
+}
+
+// Add one float64 map's E and B at a located cell; components the layout
+// does not store are identically zero and are not gathered.
+__device__ __forceinline__ void gather_map_f64(const MapDev& m, const Cell& c, V3& E, V3& B) {
+    switch (m.layout) {
+        case kLayFull:
+            E = E + gather_f64(m, c, 0);
+            B = B + gather_f64(m, c, m.b_off);
+            break;
+        case kLayE:
+            E = E + gather_f64(m, c, 0);
+            break;
+        case kLayB:
+            B = B + gather_f64(m, c, 0);
+            break;
+        case kLayExEyBz: {
+            const V3 o = gather_f64(m, c, 0);
+            E.x += o.x;
+            E.y += o.y;
+            B.z += o.z;
+            break;
+        }
+        case kLayEzBz: {
+            double o[2];
+            gather_slots_f64<2>(m, c, o);
+            E.z += o[0];
+            B.z += o[1];
+            break;
+        }
+        default: {   // kLayBz
+            double o[1];
+            gather_slots_f64<1>(m, c, o);
+            B.z += o[0];
+            break;
+        }
+    }
+}
+
 // E and B at r from all maps plus the constant parts (float64).  Returns the
 // number of maps whose grid contained r.
 __device__ __forceinline__ int eval_fields_f64(const FieldsDev& F, V3 r, V3& E, V3& B) {
@@ -217,8 +292,7 @@ __device__ __forceinline__ int eval_fields_f64(const FieldsDev& F, V3 r, V3& E, 
         Cell c;
         if (!locate(m, r, c)) continue;
         ++hits;
-        if (m.has_e) E = E + gather_f64(m, c, 0);
-        if (m.has_b) B = B + gather_f64(m, c, m.b_off);
+        gather_map_f64(m, c, E, B);
     }
     return hits;
 }

@@ -5,7 +5,8 @@
 // block of every job (the same TrackDev / TrackMixDev the single-job kernels
 // take), per-class work-queue index arrays, and per-job step counters and
 // done flags.  ppt_jobs_tick then advances every unfinished job by up to
-// `chunk` steps with one persistent kernel per (form, algorithm, RF) class --
+// `chunk` steps with one persistent kernel per (form, algorithm, RF, mixed
+// map layout) class --
 // blocks take (job, 128-particle block) items from a device queue -- followed
 // by a one-thread-per-job kernel that advances the step counters.  A tick
 // reads nothing from the host and synchronises nothing, so the host can
@@ -24,6 +25,7 @@ struct ppt_jobs {
         int precision;
         int algorithm;
         int rf;
+        int layout;   // mixed form: the map's record layout
         int grid;
         ppt::JobQueueDev Q;
     };
@@ -37,7 +39,16 @@ struct ppt_jobs {
 
 namespace ppt {
 
-constexpr int kMaxClasses = 2 * PPT_ALG_COUNT * 2;
+// classes: (form, algorithm, RF, record layout of a mixed job's map)
+constexpr int kLayouts[] = {kLayFull, kLayE, kLayB, kLayExEyBz, kLayEzBz, kLayBz};
+constexpr int kNumLayouts = 6;
+constexpr int kMaxClasses = 2 * PPT_ALG_COUNT * 2 * kNumLayouts;
+
+static int layout_index(int layout) {
+    for (int i = 0; i < kNumLayouts; ++i)
+        if (kLayouts[i] == layout) return i;
+    return 0;
+}
 
 static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -162,7 +173,8 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
         }
         reinterpret_cast<int64_t*>(img + L.steps)[j] = jobs[j].steps_done;
         const int rf = jobs[j].rf_phase != nullptr;
-        cls[j] = (jobs[j].state.precision * PPT_ALG_COUNT + jobs[j].state.algorithm) * 2 + rf;
+        const int lay = jobs[j].state.precision == PPT_PREC_MIXED ? layout_index(mix[j].map.layout) : 0;
+        cls[j] = ((jobs[j].state.precision * PPT_ALG_COUNT + jobs[j].state.algorithm) * 2 + rf) * kNumLayouts + lay;
     }
     int pos = 0, ipos = 0;
     for (int c = 0; c < kMaxClasses; ++c) {
@@ -180,9 +192,11 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
         if (pos == first) continue;
         istart[ipos++] = items;
         ppt_jobs::Class K;
-        K.precision = c / (2 * PPT_ALG_COUNT);
-        K.algorithm = (c / 2) % PPT_ALG_COUNT;
-        K.rf = c % 2;
+        const int c0 = c / kNumLayouts;
+        K.precision = c0 / (2 * PPT_ALG_COUNT);
+        K.algorithm = (c0 / 2) % PPT_ALG_COUNT;
+        K.rf = c0 % 2;
+        K.layout = kLayouts[c % kNumLayouts];
         K.grid = items < sms * 16 ? (items > 0 ? items : 1) : sms * 16;
         K.Q.table = dev + (K.precision == PPT_PREC_F64 ? L.f64 : L.mix);
         K.Q.table_index = reinterpret_cast<const int*>(dev + L.tindex) + first;
@@ -219,7 +233,7 @@ extern "C" int ppt_jobs_tick(ppt_jobs* H, int64_t chunk, void* stream) {
         JobQueueDev Q = K.Q;
         Q.chunk = chunk;
         int rc = K.precision == PPT_PREC_F64 ? launch_f64_jobs(Q, K.algorithm, K.rf != 0, K.grid, s)
-                                             : launch_mixed_jobs(Q, K.algorithm, K.rf != 0, K.grid, s);
+                                             : launch_mixed_jobs(Q, K.algorithm, K.layout, K.rf != 0, K.grid, s);
         if (rc) return rc;
     }
     jobs_advance_kernel<<<(H->n_jobs + 255) / 256, 256, 0, s>>>(H->n_jobs, H->d_steps, H->d_done, H->d_total, chunk);

@@ -44,12 +44,21 @@ __device__ __forceinline__ float tri8(Get get, float tx, float ty, float tz) {
     return lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
 }
 
-// Trilinear E/B at (cell, offset) from the float32 map; returns false when
-// outside (fields = the constant parts only).
+// Trilinear E/B at (cell, offset) from the float32 map of record layout L;
+// returns false when outside.  Components L does not store are compile-time
+// zeros, so the arithmetic that would multiply them vanishes from the
+// kernel.  Only the six-component layout carries the constant field parts
+// (the host creates that layout whenever they are not zero).
+template <int L>
 __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3], F3& E,
                                              F3& B) {
-    E = f3(P.e_const[0], P.e_const[1], P.e_const[2]);
-    B = f3(P.b_const[0], P.b_const[1], P.b_const[2]);
+    if constexpr (L == kLayFull) {
+        E = f3(P.e_const[0], P.e_const[1], P.e_const[2]);
+        B = f3(P.b_const[0], P.b_const[1], P.b_const[2]);
+    } else {
+        E = f3(0.0f, 0.0f, 0.0f);
+        B = f3(0.0f, 0.0f, 0.0f);
+    }
     int i, j, k;
     float tx, ty, tz;
     if (!mixed_axis(cell[0], f[0], P.G.n[0], i, tx)) return false;
@@ -62,14 +71,15 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     const float a00 = ux * uy, a01 = ux * ty, a10 = tx * uy, a11 = tx * ty;
     const float w[8] = {a00 * uz, a00 * tz, a01 * uz, a01 * tz, a10 * uz, a10 * tz, a11 * uz, a11 * tz};
     const int64_t node = (int64_t)i * m.sx + (int64_t)j * m.sy + k;
-    if (m.stride == 8) {
-        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner; the k+1
-        // corner is the next record (immediate offset)
-        const float* p00 = static_cast<const float*>(m.data) + node * 8;
-        const float* p10 = p00 + m.sx * 8;
-        const float* p01 = p00 + m.sy * 8;
-        const float* p11 = p10 + m.sy * 8;
-        const float* pc[4] = {p00, p01, p10, p11};   // (di, dj) = (0,0) (0,1) (1,0) (1,1)
+    constexpr int W = layout_width(L);
+    // corner (di, dj) = (0,0) (0,1) (1,0) (1,1); the k+1 corner is the next record
+    const float* p00 = static_cast<const float*>(m.data) + node * W;
+    const float* p10 = p00 + m.sx * W;
+    const float* p01 = p00 + m.sy * W;
+    const float* p11 = p10 + m.sy * W;
+    const float* pc[4] = {p00, p01, p10, p11};
+    if constexpr (L == kLayFull) {
+        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner
         float q[8][8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -87,37 +97,72 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
         }
         E = E + f3(acc[0], acc[1], acc[2]);
         B = B + f3(acc[3], acc[4], acc[5]);
-    } else {
-        // [F 0]: one 128-bit load per corner
-        const float* p00 = static_cast<const float*>(m.data) + node * 4;
-        const float* p10 = p00 + m.sx * 4;
-        const float* p01 = p00 + m.sy * 4;
-        const float* p11 = p10 + m.sy * 4;
-        const float* pc[4] = {p00, p01, p10, p11};
+    } else if constexpr (W == 4) {
+        // three packed components and a pad: one 128-bit load per corner
         float4 q[8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             q[2 * c] = __ldg(reinterpret_cast<const float4*>(pc[c]));
             q[2 * c + 1] = __ldg(reinterpret_cast<const float4*>(pc[c] + 4));
         }
-        float ox = w[0] * q[0].x, oy = w[0] * q[0].y, oz = w[0] * q[0].z;
+        float o0 = w[0] * q[0].x, o1 = w[0] * q[0].y, o2 = w[0] * q[0].z;
 #pragma unroll
         for (int c = 1; c < 8; ++c) {
-            ox = fmaf(w[c], q[c].x, ox);
-            oy = fmaf(w[c], q[c].y, oy);
-            oz = fmaf(w[c], q[c].z, oz);
+            o0 = fmaf(w[c], q[c].x, o0);
+            o1 = fmaf(w[c], q[c].y, o1);
+            o2 = fmaf(w[c], q[c].z, o2);
         }
-        if (m.has_e) E = E + f3(ox, oy, oz); else B = B + f3(ox, oy, oz);
+        if constexpr (L == kLayE) E = f3(o0, o1, o2);
+        else if constexpr (L == kLayB) B = f3(o0, o1, o2);
+        else {   // kLayExEyBz
+            E = f3(o0, o1, 0.0f);
+            B = f3(0.0f, 0.0f, o2);
+        }
+    } else if constexpr (W == 2) {
+        // kLayEzBz: one 64-bit load per corner
+        float2 q[8];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            q[2 * c] = __ldg(reinterpret_cast<const float2*>(pc[c]));
+            q[2 * c + 1] = __ldg(reinterpret_cast<const float2*>(pc[c] + 2));
+        }
+        float o0 = w[0] * q[0].x, o1 = w[0] * q[0].y;
+#pragma unroll
+        for (int c = 1; c < 8; ++c) {
+            o0 = fmaf(w[c], q[c].x, o0);
+            o1 = fmaf(w[c], q[c].y, o1);
+        }
+        E = f3(0.0f, 0.0f, o0);
+        B = f3(0.0f, 0.0f, o1);
+    } else {
+        // kLayBz: one 32-bit load per corner
+        float q[8];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            q[2 * c] = __ldg(pc[c]);
+            q[2 * c + 1] = __ldg(pc[c] + 1);
+        }
+        float o = w[0] * q[0];
+#pragma unroll
+        for (int c = 1; c < 8; ++c) o = fmaf(w[c], q[c], o);
+        B = f3(0.0f, 0.0f, o);
     }
     return true;
 }
 
+// Constant field parts exist only with the six-component layout.
+template <int L>
+__device__ __forceinline__ bool const_fields(const TrackMixDev& P) {
+    if constexpr (L == kLayFull) return P.const_nz != 0;
+    else return false;
+}
+
 // Fields at the step's field time t0 + g dt (+ toff for RK4 stages); the
 // float64 time and phase are formed only when E is non-zero.
-template <bool RF>
+template <bool RF, int L>
 __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], int64_t g,
                                              double toff, F3& E, F3& B) {
-    bool in = gather_mixed(*c.P, cell, f, E, B);
+    bool in = gather_mixed<L>(*c.P, cell, f, E, B);
     c.hits += in;
     if (RF) {
         if (E.x != 0.0f || E.y != 0.0f || E.z != 0.0f) {
@@ -132,7 +177,7 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
             E = cf * E;
         }
     }
-    return in || c.P->const_nz;
+    return in || const_fields<L>(*c.P);
 }
 
 // Boris velocity increment in float32 (pusher.py:149-163 rearranged):
@@ -317,7 +362,7 @@ __device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cn[
 // One step g of the Boris family with float-valued cell indices (exact
 // integers below 2^24).  Returns the number of following steps known to be
 // field-free (0 when this step met a field or the particle may come back).
-template <int ALG, bool RF>
+template <int ALG, bool RF, int L>
 __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
                                            int64_t g) {
     const TrackMixDev& P = *c.P;
@@ -332,10 +377,10 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], f
     // exact bounds rule is applied inside gather_mixed
     const bool maybe = (cn[0] >= 0.0f) & (cn[0] <= P.cell_max[0]) & (cn[1] >= 0.0f) & (cn[1] <= P.cell_max[1]) &
                        (cn[2] >= 0.0f) & (cn[2] <= P.cell_max[2]);
-    if (maybe || P.const_nz) {
+    if (maybe || const_fields<L>(P)) {
         const int cell[3] = {(int)cn[0], (int)cn[1], (int)cn[2]};
         F3 E, B;
-        if (fields_mixed<RF>(c, cell, fn, g, 0.0, E, B)) {
+        if (fields_mixed<RF, L>(c, cell, fn, g, 0.0, E, B)) {
             F3 v = f3(vh[0], vh[1], vh[2]);
             vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
             increment(P, vh, vl, d.dh, d.dl);
@@ -358,14 +403,14 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], f
     return quiet_steps(P, cn, fn, d.dh);
 }
 
-template <int ALG, bool RF>
+template <int ALG, bool RF, int L>
 __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float vh[3], float vl[3], Drift& d,
                                            int64_t g) {
     const TrackMixDev& P = *c.P;
     F3 v = f3(vh[0], vh[1], vh[2]);
     if constexpr (ALG == PPT_ALG_VAY_REL) {
         F3 E, B;
-        fields_mixed<RF>(c, cell, f, g, 0.0, E, B);
+        fields_mixed<RF, L>(c, cell, f, g, 0.0, E, B);
         F3 vn = vay_rel_f(v, E, B, P.qm, P.dtf);
         // increment relative to the float32 head keeps the low part's bits
         vel_add(vh, vl, vn - v);
@@ -376,19 +421,19 @@ __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], f
         F3 E, B;
         int sc[3];
         float sf[3];
-        fields_mixed<RF>(c, cell, f, g, 0.0, E, B);
+        fields_mixed<RF, L>(c, cell, f, g, 0.0, E, B);
         F3 k1 = REL ? rk4_rel_deriv_f(v, E, B, P.qm) : lorentz_f(v, E, B, P.qm);
         F3 v2 = v + h * k1;
         offset_point(P, cell, f, h * v, sc, sf);
-        fields_mixed<RF>(c, sc, sf, g, 0.5 * P.dt, E, B);
+        fields_mixed<RF, L>(c, sc, sf, g, 0.5 * P.dt, E, B);
         F3 k2 = REL ? rk4_rel_deriv_f(v2, E, B, P.qm) : lorentz_f(v2, E, B, P.qm);
         F3 v3_ = v + h * k2;
         offset_point(P, cell, f, h * v2, sc, sf);
-        fields_mixed<RF>(c, sc, sf, g, 0.5 * P.dt, E, B);
+        fields_mixed<RF, L>(c, sc, sf, g, 0.5 * P.dt, E, B);
         F3 k3 = REL ? rk4_rel_deriv_f(v3_, E, B, P.qm) : lorentz_f(v3_, E, B, P.qm);
         F3 v4 = v + dt * k3;
         offset_point(P, cell, f, dt * v3_, sc, sf);
-        fields_mixed<RF>(c, sc, sf, g, P.dt, E, B);
+        fields_mixed<RF, L>(c, sc, sf, g, P.dt, E, B);
         F3 k4 = REL ? rk4_rel_deriv_f(v4, E, B, P.qm) : lorentz_f(v4, E, B, P.qm);
         // r_new - r = dt v + dt^2/6 (k1 + k2 + k3); v_new - v = dt/6 (k1 + 2k2 + 2k3 + k4)
         const float s6 = dt * (1.0f / 6.0f);
@@ -427,7 +472,7 @@ __device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t re
     }
 }
 
-template <int ALG, bool RF>
+template <int ALG, bool RF, int L>
 __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, int64_t s, MixCtx& c) {
     {
         const int64_t n = P.n;
@@ -445,7 +490,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
-                if (fields_mixed<RF>(c, cell, f, P.step0, 0.0, E, B))
+                if (fields_mixed<RF, L>(c, cell, f, P.step0, 0.0, E, B))
                     // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
                     vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt));
             }
@@ -473,7 +518,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                         i += m;
                         quiet -= m;
                     } else {
-                        quiet = family_step<ALG, RF>(c, cf, f, vh, vl, d, g0 + i);
+                        quiet = family_step<ALG, RF, L>(c, cf, f, vh, vl, d, g0 + i);
                         ++i;
                     }
                 }
@@ -492,7 +537,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             for (int a = 0; a < 3; ++a) cell[a] = (int)cf[a];
         } else {
             for (int k = 0; k < nsteps; ++k) {
-                mixed_step<ALG, RF>(c, cell, f, vh, vl, d, P.step0 + k);
+                mixed_step<ALG, RF, L>(c, cell, f, vh, vl, d, P.step0 + k);
                 if (until == 0) {
                     const int64_t rec = (P.step0 + k + 1) / P.rec_every;
                     if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, vh, vl, true);
@@ -513,7 +558,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                     cn[a] = cell[a] + (int)cc;
                     fn[a] = f[a] - cc;
                 }
-                if (fields_mixed<RF>(c, cn, fn, P.nsteps_total, 0.0, E, B))
+                if (fields_mixed<RF, L>(c, cn, fn, P.nsteps_total, 0.0, E, B))
                     // Boris push with time step +dt/2 (pusher.py:993-1007)
                     vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt));
                 if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
@@ -536,19 +581,19 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
     return (unsigned)P.nsteps;
 }
 
-template <int ALG, bool RF>
+template <int ALG, bool RF, int L>
 __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
     MixCtx c{&P, 0.0, 0u};
-    if (s < P.n) steps_done = track_mixed_particle<ALG, RF>(P, s, c);
+    if (s < P.n) steps_done = track_mixed_particle<ALG, RF, L>(P, s, c);
     if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
 }
 
 // Serving: the mixed-precision counterpart of track_f64_jobs_kernel.
 static_assert(sizeof(TrackMixDev) % 8 == 0, "TrackMixDev is copied as 8-byte words");
 
-template <int ALG, bool RF>
+template <int ALG, bool RF, int L>
 __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __grid_constant__ JobQueueDev Q) {
     __shared__ __align__(16) TrackMixDev sP;
     __shared__ int s_item, s_job;
@@ -578,59 +623,67 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
             MixCtx c{&sP, 0.0, 0u};
             unsigned sd = 0;
-            if (s < sP.n) sd = track_mixed_particle<ALG, RF>(sP, s, c);
+            if (s < sP.n) sd = track_mixed_particle<ALG, RF, L>(sP, s, c);
             if (sP.counters) block_add_counters(sP.counters, c.hits, sd);
         }
         __syncthreads();
     }
 }
 
-template <int ALG>
-static cudaError_t launch_mixed_jobs_alg(const JobQueueDev& Q, bool rf, int grid, cudaStream_t s) {
-    if (rf) track_mixed_jobs_kernel<ALG, true><<<grid, kJobBlock, 0, s>>>(Q);
-    else track_mixed_jobs_kernel<ALG, false><<<grid, kJobBlock, 0, s>>>(Q);
+// Kernel of (algorithm, RF, layout).  Layouts without E ignore the RF flag:
+// their fields have no E to modulate.
+template <int ALG, int L>
+static cudaError_t launch_mixed_layout(const TrackMixDev* P, const JobQueueDev* Q, bool rf, int grid,
+                                       cudaStream_t s) {
+    constexpr bool kE = layout_has_e(L);
+    if (P) {
+        const int block = pick_block(P->n);
+        const int g = grid_for(P->n, block);
+        if (rf && kE) track_mixed_kernel<ALG, kE, L><<<g, block, 0, s>>>(*P);
+        else track_mixed_kernel<ALG, false, L><<<g, block, 0, s>>>(*P);
+    } else {
+        if (rf && kE) track_mixed_jobs_kernel<ALG, kE, L><<<grid, kJobBlock, 0, s>>>(*Q);
+        else track_mixed_jobs_kernel<ALG, false, L><<<grid, kJobBlock, 0, s>>>(*Q);
+    }
     return cudaGetLastError();
 }
 
-int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s) {
+template <int ALG>
+static cudaError_t launch_mixed_alg(const TrackMixDev* P, const JobQueueDev* Q, int layout, bool rf, int grid,
+                                    cudaStream_t s) {
+    switch (layout) {
+        case kLayFull: return launch_mixed_layout<ALG, kLayFull>(P, Q, rf, grid, s);
+        case kLayE: return launch_mixed_layout<ALG, kLayE>(P, Q, rf, grid, s);
+        case kLayB: return launch_mixed_layout<ALG, kLayB>(P, Q, rf, grid, s);
+        case kLayExEyBz: return launch_mixed_layout<ALG, kLayExEyBz>(P, Q, rf, grid, s);
+        case kLayEzBz: return launch_mixed_layout<ALG, kLayEzBz>(P, Q, rf, grid, s);
+        default: return launch_mixed_layout<ALG, kLayBz>(P, Q, rf, grid, s);
+    }
+}
+
+static int launch_mixed(const TrackMixDev* P, const JobQueueDev* Q, int algorithm, int layout, bool rf, int grid,
+                        cudaStream_t s, const char* what) {
     cudaError_t e;
     switch (algorithm) {
-        case PPT_ALG_LEAPFROG: e = launch_mixed_jobs_alg<PPT_ALG_LEAPFROG>(Q, rf, grid, s); break;
-        case PPT_ALG_BORIS: e = launch_mixed_jobs_alg<PPT_ALG_BORIS>(Q, rf, grid, s); break;
-        case PPT_ALG_RK4: e = launch_mixed_jobs_alg<PPT_ALG_RK4>(Q, rf, grid, s); break;
-        case PPT_ALG_VAY_REL: e = launch_mixed_jobs_alg<PPT_ALG_VAY_REL>(Q, rf, grid, s); break;
-        case PPT_ALG_RK4_REL: e = launch_mixed_jobs_alg<PPT_ALG_RK4_REL>(Q, rf, grid, s); break;
+        case PPT_ALG_LEAPFROG: e = launch_mixed_alg<PPT_ALG_LEAPFROG>(P, Q, layout, rf, grid, s); break;
+        case PPT_ALG_BORIS: e = launch_mixed_alg<PPT_ALG_BORIS>(P, Q, layout, rf, grid, s); break;
+        case PPT_ALG_RK4: e = launch_mixed_alg<PPT_ALG_RK4>(P, Q, layout, rf, grid, s); break;
+        case PPT_ALG_VAY_REL: e = launch_mixed_alg<PPT_ALG_VAY_REL>(P, Q, layout, rf, grid, s); break;
+        case PPT_ALG_RK4_REL: e = launch_mixed_alg<PPT_ALG_RK4_REL>(P, Q, layout, rf, grid, s); break;
         default:
             return fail(PPT_ERR_UNSUPPORTED,
                         "the mixed form covers leapfrog, boris, rk4, vay_rel and rk4_rel; use precision 'fp64'");
     }
-    if (e != cudaSuccess) return cuda_fail(e, "track_mixed_jobs_kernel launch");
+    if (e != cudaSuccess) return cuda_fail(e, what);
     return PPT_OK;
 }
 
-template <int ALG>
-static cudaError_t launch_mixed_alg(const TrackMixDev& P, bool rf, cudaStream_t s) {
-    const int block = pick_block(P.n);
-    const int grid = grid_for(P.n, block);
-    if (rf) track_mixed_kernel<ALG, true><<<grid, block, 0, s>>>(P);
-    else track_mixed_kernel<ALG, false><<<grid, block, 0, s>>>(P);
-    return cudaGetLastError();
+int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, int layout, bool rf, int grid, cudaStream_t s) {
+    return launch_mixed(nullptr, &Q, algorithm, layout, rf, grid, s, "track_mixed_jobs_kernel launch");
 }
 
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s) {
-    cudaError_t e;
-    switch (algorithm) {
-        case PPT_ALG_LEAPFROG: e = launch_mixed_alg<PPT_ALG_LEAPFROG>(P, rf, s); break;
-        case PPT_ALG_BORIS: e = launch_mixed_alg<PPT_ALG_BORIS>(P, rf, s); break;
-        case PPT_ALG_RK4: e = launch_mixed_alg<PPT_ALG_RK4>(P, rf, s); break;
-        case PPT_ALG_VAY_REL: e = launch_mixed_alg<PPT_ALG_VAY_REL>(P, rf, s); break;
-        case PPT_ALG_RK4_REL: e = launch_mixed_alg<PPT_ALG_RK4_REL>(P, rf, s); break;
-        default:
-            return fail(PPT_ERR_UNSUPPORTED,
-                        "the mixed form covers leapfrog, boris, rk4, vay_rel and rk4_rel; use precision 'fp64'");
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "track_mixed_kernel launch");
-    return PPT_OK;
+    return launch_mixed(&P, nullptr, algorithm, P.map.layout, rf, 0, s, "track_mixed_kernel launch");
 }
 
 // host-side construction of the mixed kernel parameters
@@ -649,6 +702,10 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
         P->cell_max[c] = (float)(P->G.n[c] - 1);
     }
     P->const_nz = F.e_const_nz || F.b_const_nz;
+    if (P->const_nz && P->map.layout != kLayFull)
+        return fail(PPT_ERR_UNSUPPORTED,
+                    "mixed form: fields with constant parts need a map of all six components "
+                    "(ppt_fieldmap_create_masked with 0x3F)");
     P->n = st->n;
     P->step0 = a->step0;
     P->nsteps = a->nsteps;

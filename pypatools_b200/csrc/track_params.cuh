@@ -88,7 +88,7 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
                      TrackMixDev* P);
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s);
 int launch_f64_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s);
-int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s);
+int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, int layout, bool rf, int grid, cudaStream_t s);
 
 // Device helper shared by both job kernels: thread 0 takes the next item and
 // finds its class-local job by bisection over item_start.

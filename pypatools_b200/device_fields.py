@@ -20,7 +20,10 @@ Anything else raises ``NotImplementedError``: there is no CPU fallback.
 
 Terms on the same node grid are summed into one device map; when E and B
 share a grid they share one map, so each step does one cell lookup and one
-gather of [E | B] node records.
+gather of [E | B] node records.  Components that are identically zero in
+every term (an RF gap's Ex, Ey, Bx, By; a sector magnet's Bx, By) are not
+stored: the map's records keep only the others (``ppt_fieldmap_create_masked``),
+which the kernels then neither gather nor multiply.
 """
 import weakref
 
@@ -81,17 +84,24 @@ _zero_cache = {}
 
 
 def _all_zero(values):
-    """True when a node array is identically zero; remembered per buffer
-    (address, shape, dtype) so repeated cache lookups do not rescan maps."""
+    """True when a node array is identically zero.  Remembered per array
+    object (validated through a weak reference, so an array allocated later
+    at a freed one's address is scanned afresh); node arrays are treated as
+    immutable once a field uses them."""
     a = np.asarray(values)
-    key = (a.__array_interface__["data"][0], a.shape, a.dtype.str)
+    key = id(a)
     hit = _zero_cache.get(key)
-    if hit is None:
-        hit = not np.any(a)
-        if len(_zero_cache) > 4096:
-            _zero_cache.clear()
-        _zero_cache[key] = hit
-    return hit
+    if hit is not None and hit[0]() is a:
+        return hit[1]
+    result = not np.any(a)
+    try:
+        ref = weakref.ref(a)
+    except TypeError:
+        return result
+    if len(_zero_cache) > 4096:
+        _zero_cache.clear()
+    _zero_cache[key] = (ref, result)
+    return result
 
 
 def decompose(field):
@@ -152,7 +162,7 @@ def _grid_key(grid):
 class DeviceFields:
     """Device maps + constants for one (efield, bfield, precision) triple."""
 
-    def __init__(self, efield, bfield, precision="fp64", device=None):
+    def __init__(self, efield, bfield, precision="fp64", device=None, prune=True):
         import torch
         self._torch = torch
         lib = _lib.load()
@@ -169,26 +179,42 @@ class DeviceFields:
         if len(groups) > _lib.MAX_MAPS:
             raise NotImplementedError(f"at most {_lib.MAX_MAPS} distinct node grids per pusher call")
         self.maps = []
+        self.layouts = []
         self.map_bytes = 0
         self.n_components = 0
+        has_const = bool(np.any(e_terms.const != 0.0) or np.any(b_terms.const != 0.0))
         with torch.cuda.device(self.device):
             stream = _lib.stream_handle()
             for g in groups.values():
+                mask = 0
+                for kind, base in (("e", 0), ("b", 3)):
+                    for t in g[kind]:
+                        for ci, c in enumerate("xyz"):
+                            a = t.comps.get(c)
+                            if a is not None and not _all_zero(a):
+                                mask |= 1 << (base + ci)
+                if mask == 0:
+                    continue     # every term of this grid is zero
+                if not prune:
+                    mask = (0x07 if g["e"] else 0) | (0x38 if g["b"] else 0)
+                if precision == "mixed" and has_const:
+                    mask = _lib.FULL_MASK   # the mixed kernels take constant parts with this layout only
                 handle = ctypes_void()
                 desc = _lib.GridDesc()
                 axes = [np.ascontiguousarray(a, dtype=np.float64) for a in g["grid"]]
                 for d in range(3):
                     desc.n[d] = axes[d].shape[0]
                     desc.axis[d] = axes[d].ctypes.data
-                _lib.check(lib.ppt_fieldmap_create(desc, int(bool(g["e"])), int(bool(g["b"])), store, handle))
+                _lib.check(lib.ppt_fieldmap_create_masked(desc, mask, store, handle))
                 self.maps.append(handle.value)
                 for kind in ("e", "b"):
                     for t in g[kind]:
-                        self._add_term(lib, handle.value, kind, t, stream)
-                nbytes = _lib.c_int64()
-                _lib.check(lib.ppt_fieldmap_info(handle.value, nbytes, None))
+                        self._add_term(lib, handle.value, kind, t, stream, mask)
+                nbytes, flags = _lib.c_int64(), _lib.c_int()
+                _lib.check(lib.ppt_fieldmap_info(handle.value, nbytes, flags))
                 self.map_bytes += nbytes.value
-                self.n_components += 3 * (int(bool(g["e"])) + int(bool(g["b"])))
+                self.layouts.append((flags.value >> 8) & 0x3F)
+                self.n_components += bin(mask).count("1")
             torch.cuda.current_stream().synchronize()
         self.fields = _lib.Fields()
         for i, h in enumerate(self.maps):
@@ -201,11 +227,14 @@ class DeviceFields:
         self.b_const = b_terms.const.copy()
         self._finalizer = weakref.finalize(self, _destroy_maps, list(self.maps))
 
-    def _add_term(self, lib, handle, kind, term, stream):
+    def _add_term(self, lib, handle, kind, term, stream, mask):
         torch = self._torch
         ptrs = (_lib.c_void_p * 6)()
         scales = (_lib.c_double * 6)()
-        present = [(ci, np.asarray(term.comps[c])) for ci, c in enumerate("xyz") if term.comps.get(c) is not None]
+        base = 0 if kind == "e" else 3
+        # components outside the mask are identically zero: nothing to add
+        present = [(ci, np.asarray(term.comps[c])) for ci, c in enumerate("xyz")
+                   if term.comps.get(c) is not None and mask & (1 << (base + ci))]
         if not present:
             return
         # float32 node values stay float32 (exact); anything else goes as float64

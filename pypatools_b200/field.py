@@ -113,7 +113,7 @@ class Field(FieldBase):
         points = [np.asarray(grid[k], dtype=np.float64) for k in "xyz" if k in grid and len(grid[k]) > 1]
         field._dim = len(points)
         for c in "xyz":
-            if c in values:
+            if values.get(c) is not None:
                 field._field[c] = get_interpolator(tuple(points), values[c], method=field._method,
                                                    bounds_error=False, fill_value=0.0,
                                                    backend=field._interpolator_backend)

@@ -70,6 +70,28 @@ def test_capi_argument_errors_without_gpu():
     assert lib.ppt_track(st, _lib.Fields(), a, None) == 0
 
 
+def test_map_layout_choice_without_gpu():
+    # smallest compiled layout containing the stored components
+    lib = _lib.load()
+    bz, ez, ex, ey, bx, by = 0x20, 0x04, 0x01, 0x02, 0x08, 0x10
+    assert lib.ppt_fieldmap_layout(bz) == bz                      # sector magnet: Bz only
+    assert lib.ppt_fieldmap_layout(ez | bz) == ez | bz            # RF gap + solenoid
+    assert lib.ppt_fieldmap_layout(ez) == ez | bz
+    assert lib.ppt_fieldmap_layout(ex | ey | bz) == ex | ey | bz  # radial E + solenoid
+    assert lib.ppt_fieldmap_layout(bx | by | bz) == bx | by | bz  # quadrupole + solenoid
+    assert lib.ppt_fieldmap_layout(by) == bx | by | bz
+    assert lib.ppt_fieldmap_layout(ex) == ex | ey | ez
+    assert lib.ppt_fieldmap_layout(ex | by) == 0x3F
+    assert lib.ppt_fieldmap_layout(ez | bx) == 0x3F
+    assert lib.ppt_fieldmap_layout(0) == -1
+    assert lib.ppt_fieldmap_layout(0x40) == -1
+    out = ctypes.c_void_p()
+    assert lib.ppt_fieldmap_create_masked(None, 0x20, _lib.DTYPE_F32, out) == -1
+    g = _lib.GridDesc()
+    assert lib.ppt_fieldmap_create_masked(g, 0, _lib.DTYPE_F32, out) == -1
+    assert b"comp_mask" in lib.ppt_last_error()
+
+
 def test_check_raises_with_message():
     lib = _lib.load()
     with pytest.raises(_lib.PptError, match="PPT_ERR_ARG"):
