@@ -23,9 +23,52 @@ constexpr double kInvTwoPi = 0.15915494309189535;
 
 struct MixCtx {
     const TrackMixDev* P;
-    double phase;
+    double phase;            // omega t0 + phi_i
     unsigned hits;
+    double c0, s0;           // cos, sin of the phase
+    const double2* tab;      // (cos, sin) of g omega dt for g = tab0 .. tab0 + tab_n - 1, or NULL
+    int64_t tab0;
+    int tab_n;
 };
+
+// Per-step RF table length limit: the sorted launches of a bunch crossing
+// its map are ~100 steps; longer launches compute the same values directly.
+constexpr int kRfTable = 512;
+
+// (cos, sin) of g omega dt in float64: the per-step factor of the RF phase,
+// the same for every particle, so a block tabulates it once per launch.
+__device__ __forceinline__ void rf_turn(int64_t g, double wdt, double& cg, double& sg) {
+    sincos((double)g * wdt, &sg, &cg);
+}
+
+// cos(omega (t0 + g dt) + phi_i) = cos(a + b) = cos a cos b - sin a sin b
+// with a = omega t0 + phi_i per particle and b = g omega dt per step, in
+// float64 and rounded once to float32.  The value depends on g and the
+// particle only (table or not), so tracks split into launches differently
+// agree bit for bit.
+__device__ __forceinline__ float rf_cos(const MixCtx& c, int64_t g) {
+    double cg, sg;
+    const int64_t k = g - c.tab0;
+    if (c.tab != nullptr && k >= 0 && k < c.tab_n) {
+        const double2 t = c.tab[k];
+        cg = t.x;
+        sg = t.y;
+    } else {
+        rf_turn(g, c.P->wdt, cg, sg);
+    }
+    return (float)fma(c.c0, cg, -(c.s0 * sg));
+}
+
+// Fill the block's RF table for steps step0 .. step0 + n - 1 (all threads
+// of the block call it; n <= kRfTable).
+__device__ __forceinline__ void build_rf_table(double2* tab, int64_t step0, int n, double wdt) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double cg, sg;
+        rf_turn(step0 + i, wdt, cg, sg);
+        tab[i] = make_double2(cg, sg);
+    }
+    __syncthreads();
+}
 
 // 256-bit read-only load of one [E | B] node record (32-B aligned).
 __device__ __forceinline__ void ldg_f32x8(const float* p, float (&v)[8]) {
@@ -167,13 +210,18 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
     if (RF) {
         if (E.x != 0.0f || E.y != 0.0f || E.z != 0.0f) {
             // omega (t0 + g dt + toff) + phi_i = (omega t0 + phi_i) + g (omega dt) + omega toff, in float64
-            double ph = fma((double)g, c.P->wdt, c.phase);
-            if (toff != 0.0) ph = fma(c.P->omega, toff, ph);
-            double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
-            // the argument is already in [-pi, pi], so cosf takes its short
-            // path; the hardware __cosf (absolute error 2^-21.4, six times the
-            // float32 rounding of the field values) doubled the error tail
-            float cf = cosf((float)red);
+            float cf;
+            if (toff == 0.0) {
+                cf = rf_cos(c, g);
+            } else {
+                // RK4 stage times t + dt/2, t + dt: the phase reduced to
+                // [-pi, pi] in float64, then cosf (the hardware __cosf,
+                // absolute error 2^-21.4, doubled the error tail)
+                double ph = fma((double)g, c.P->wdt, c.phase);
+                ph = fma(c.P->omega, toff, ph);
+                const double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
+                cf = cosf((float)red);
+            }
             E = cf * E;
         }
     }
@@ -486,7 +534,10 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             vl[a] = P.fs[(6 + a) * n + s];
         }
         const int64_t row = P.order ? P.order[s] : s;
-        if (RF) c.phase = fma(P.omega, P.t0, P.rf_phase[s]);   // omega t0 + phi_i
+        if (RF) {
+            c.phase = fma(P.omega, P.t0, P.rf_phase[s]);   // omega t0 + phi_i
+            sincos(c.phase, &c.s0, &c.c0);
+        }
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
@@ -585,7 +636,16 @@ template <int ALG, bool RF, int L>
 __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u};
+    MixCtx c{&P, 0.0, 0u, 0.0, 0.0, nullptr, 0, 0};
+    if constexpr (RF) {
+        extern __shared__ double2 rf_tab[];
+        if (P.rf_tab_n > 0) {
+            build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
+            c.tab = rf_tab;
+            c.tab0 = P.step0;
+            c.tab_n = P.rf_tab_n;
+        }
+    }
     if (s < P.n) steps_done = track_mixed_particle<ALG, RF, L>(P, s, c);
     if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
 }
@@ -621,7 +681,18 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
         __syncthreads();
         if (sP.flags >= 0) {
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
-            MixCtx c{&sP, 0.0, 0u};
+            MixCtx c{&sP, 0.0, 0u, 0.0, 0.0, nullptr, 0, 0};
+            if constexpr (RF) {
+                // this job's step window, when the launch reserved a table for it
+                extern __shared__ double2 rf_tab[];
+                const int nt = (int)sP.nsteps + 1;
+                if (Q.chunk + 1 <= kRfTable && nt <= kRfTable) {
+                    build_rf_table(rf_tab, sP.step0, nt, sP.wdt);
+                    c.tab = rf_tab;
+                    c.tab0 = sP.step0;
+                    c.tab_n = nt;
+                }
+            }
             unsigned sd = 0;
             if (s < sP.n) sd = track_mixed_particle<ALG, RF, L>(sP, s, c);
             if (sP.counters) block_add_counters(sP.counters, c.hits, sd);
@@ -639,10 +710,12 @@ static cudaError_t launch_mixed_layout(const TrackMixDev* P, const JobQueueDev* 
     if (P) {
         const int block = pick_block(P->n);
         const int g = grid_for(P->n, block);
-        if (rf && kE) track_mixed_kernel<ALG, kE, L><<<g, block, 0, s>>>(*P);
+        const size_t smem = (size_t)P->rf_tab_n * sizeof(double2);
+        if (rf && kE) track_mixed_kernel<ALG, kE, L><<<g, block, smem, s>>>(*P);
         else track_mixed_kernel<ALG, false, L><<<g, block, 0, s>>>(*P);
     } else {
-        if (rf && kE) track_mixed_jobs_kernel<ALG, kE, L><<<grid, kJobBlock, 0, s>>>(*Q);
+        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(double2) : 0;
+        if (rf && kE) track_mixed_jobs_kernel<ALG, kE, L><<<grid, kJobBlock, smem, s>>>(*Q);
         else track_mixed_jobs_kernel<ALG, false, L><<<grid, kJobBlock, 0, s>>>(*Q);
     }
     return cudaGetLastError();
@@ -721,6 +794,10 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
     P->hqdt = (float)(0.5 * a->q_over_m * a->dt);
     P->dtf = (float)a->dt;
     P->rf_phase = a->rf_phase;
+    // the launch's per-step RF table covers steps step0 .. step0 + nsteps
+    // (the closing half step reads the last one)
+    P->rf_tab_n = (a->rf_phase && a->nsteps + 1 <= kRfTable) ? (int32_t)(a->nsteps + 1) : 0;
+    P->pad = 0;
     P->ci = st->i32;
     P->fs = st->f32;
     P->r_hist = a->r_hist;

@@ -60,6 +60,8 @@ struct TrackMixDev {
     const int64_t* order;
     int* status;
     unsigned long long* counters;
+    int32_t rf_tab_n;   // entries of the per-step RF table a launch builds (0: none)
+    int32_t pad;
 };
 
 // One (form, algorithm, RF) class of serving jobs: a block-level work queue
