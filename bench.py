@@ -37,8 +37,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=10_000_000)
-    ap.add_argument("--nsteps", type=int, default=20_000)
+    ap.add_argument("--workload", choices=["rf_gap", "pusher_sweep", "sector_ring"], default="rf_gap",
+                    help="rf_gap: the headline line (default); pusher_sweep: 1e6 electrons, Boris / vay_rel "
+                         "/ rk4_rel in both forms; sector_ring: 1e8 protons on a 512^3 Bz map")
+    ap.add_argument("--n", type=int, default=None, help="particles (default: the workload's)")
+    ap.add_argument("--nsteps", type=int, default=None, help="steps per job (default: the workload's)")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -48,13 +51,139 @@ def parse():
                     help="cell re-sort interval in steps (also the launch length); 0 = never")
     ap.add_argument("--serve-jobs", type=int, default=300,
                     help="jobs of the serving stream per form (2000 = the full stream); 0 skips it")
-    return ap.parse_args()
+    args = ap.parse_args()
+    defaults = {"rf_gap": (10_000_000, 20_000), "pusher_sweep": (1_000_000, 10_000),
+                "sector_ring": (100_000_000, 50_000)}[args.workload]
+    args.n = args.n or defaults[0]
+    args.nsteps = args.nsteps or defaults[1]
+    return args
 
 
 # DRAM bytes per particle per launch of the mixed track kernel, from the ncu
 # capture of a 100-step in-map launch on the RF-gap workload at 1e6 protons
 # (the state read and written; the map's occupied cells stay in L2).
 MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 66.5
+
+
+def _timed_track(tr, r0, v0, nsteps, sort_every, phase=None):
+    """Load and run one whole track; device milliseconds."""
+    import torch
+    tr.step = 0
+    tr.order = None
+    if phase is not None:
+        tr.rf_phase.copy_(phase)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    tr.load(r0, v0)
+    tr.run(nsteps, sort_every or nsteps, sort_every=sort_every)
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def _rel_err(r, r64, floor):
+    """Per-particle worst |r - r64| / max(|r64|, floor) over the records."""
+    import torch
+    num = torch.linalg.vector_norm(r - r64, dim=-1)
+    den = torch.clamp(torch.linalg.vector_norm(r64, dim=-1), min=floor)
+    rel = (num / den).amax(dim=0)
+    srt = torch.sort(rel.flatten()).values
+    q = lambda p: float(srt[min(srt.numel() - 1, int(p * srt.numel()))])
+    return {"p50": q(0.5), "p99": q(0.99), "max": float(srt[-1]), "over_1e-6": int((srt > 1e-6).sum())}
+
+
+def run_pusher_sweep(args, dev):
+    """1e6 electrons (10 keV-10 MeV, isotropic) in a radial 1 MV/m E and a
+    0.5 T cos(pi z / 0.2 m) solenoid B on a 129^3 map, dt = 1e-12 s, 1e4
+    steps: Boris, vay_rel and rk4_rel in both forms, the mixed form's error
+    against the float64 form (which matches the oracle to 1e-10)."""
+    import torch
+    from pypatools_b200 import workloads, Field
+    from pypatools_b200.device_fields import DeviceFields
+    from pypatools_b200.pusher import DeviceTracker
+    wl = workloads.radial_e_solenoid_electrons(n=args.n, nsteps=args.nsteps)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    ef, bf = Field.from_arrays(g, wl.e_values), Field.from_arrays(g, wl.b_values)
+    r0, v0 = torch.from_numpy(wl.r0).to(dev), torch.from_numpy(wl.v0).to(dev)
+    out = {}
+    for alg in ("boris", "vay_rel", "rk4_rel"):
+        res, hist = {}, {}
+        for form in ("fp64", "mixed"):
+            df = DeviceFields(ef, bf, form, dev)
+            tr = DeviceTracker(alg, wl.species.q_over_m, df, wl.n, wl.nsteps, wl.dt, wl.rec_every, form,
+                               device=dev)
+            warm = DeviceTracker(alg, wl.species.q_over_m, df, min(wl.n, 4096), 50, wl.dt, 50, form, device=dev)
+            _timed_track(warm, r0[:warm.n], v0[:warm.n], 50, args.sort_every)
+            ms = _timed_track(tr, r0, v0, wl.nsteps, args.sort_every)
+            res[form] = {"particle_steps_per_s": wl.n * wl.nsteps / (ms / 1e3), "ms": ms}
+            hist[form] = tr.r_hist
+            del tr, warm
+        res["mixed_over_fp64"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+        res["error_vs_fp64"] = _rel_err(hist["mixed"], hist["fp64"], 0.1)
+        out[alg] = res
+        del hist
+        torch.cuda.empty_cache()
+    return {"metric": "particle-steps/s per pusher, mixed vs float64, and the mixed form's error",
+            "workload": "radial_e_solenoid_electrons", "particles": wl.n, "steps": wl.nsteps, "dt": wl.dt,
+            "map": "129^3 over a 20 cm cube: E radial 1 MV/m at r = 0.1 m, Bz = 0.5 T cos(pi z / 0.2 m)",
+            "error_metric": "per particle max over the start and end records of |r - r64| / max(|r64|, 0.1 m)",
+            "sort_every": args.sort_every, "results": out}
+
+
+def run_sector_ring(args, dev):
+    """1e8 protons (5 MeV +-0.5 %) circulating in a four-sector Bz map
+    (512^3 float32 over a 1 m cube, 1 T (1 + 0.1 cos 4 theta) - 0.05 T/m r),
+    dt = 1e-10 s, 5e4 steps, cell re-sort every 100 steps.  Mixed form over
+    the whole job; the float64 form timed on the first 1/10 of the steps at
+    full size; the mixed form's error against the float64 form on a
+    1e5-particle subsample over the whole job."""
+    import torch
+    from pypatools_b200 import workloads, Field
+    from pypatools_b200.device_fields import DeviceFields
+    from pypatools_b200.pusher import DeviceTracker
+    wl = workloads.sector_ring_protons(n=args.n, nsteps=args.nsteps)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    bf = Field.from_arrays(g, wl.b_values)
+    r0, v0 = torch.from_numpy(wl.r0).to(dev), torch.from_numpy(wl.v0).to(dev)
+    sub = min(wl.n, 100_000)
+    qm = wl.species.q_over_m
+    out = {}
+    dfm = DeviceFields(None, bf, "mixed", dev)
+    warm = DeviceTracker("boris", qm, dfm, 4096, 50, wl.dt, 50, "mixed", device=dev)
+    _timed_track(warm, r0[:4096], v0[:4096], 50, args.sort_every)
+    tr = DeviceTracker("boris", qm, dfm, wl.n, wl.nsteps, wl.dt, wl.rec_every, "mixed", device=dev)
+    ms = _timed_track(tr, r0, v0, wl.nsteps, args.sort_every)
+    out["mixed"] = {"particle_steps_per_s": wl.n * wl.nsteps / (ms / 1e3), "ms_job": ms}
+    r_mixed_sub = tr.r_hist[:, :sub].clone()
+    del tr
+    torch.cuda.empty_cache()
+    df64 = DeviceFields(None, bf, "fp64", dev)
+    window = max(1, wl.nsteps // 10)
+    tr = DeviceTracker("boris", qm, df64, wl.n, window, wl.dt, window, "fp64", device=dev)
+    ms64 = _timed_track(tr, r0, v0, window, args.sort_every)
+    out["fp64"] = {"particle_steps_per_s": wl.n * window / (ms64 / 1e3), "ms": ms64, "steps_timed": window}
+    del tr
+    torch.cuda.empty_cache()
+    tr = DeviceTracker("boris", qm, df64, sub, wl.nsteps, wl.dt, wl.rec_every, "fp64", device=dev)
+    _timed_track(tr, r0[:sub].contiguous(), v0[:sub].contiguous(), wl.nsteps, args.sort_every)
+    out["mixed_over_fp64"] = out["mixed"]["particle_steps_per_s"] / out["fp64"]["particle_steps_per_s"]
+    out["error_vs_fp64"] = _rel_err(r_mixed_sub, tr.r_hist, 0.5)
+    out["error_vs_fp64"]["sample"] = f"first {sub} particles, whole job"
+    # particles that leave the map (no vertical focusing in a Bz-only map)
+    # fly straight on: a one-step difference in the exit makes a different line
+    end = tr.r_hist[-1]
+    inside = (end.abs() <= 0.5).all(dim=1)
+    out["left_map_fraction"] = float(1.0 - inside.double().mean())
+    if bool(inside.any()):
+        e_in = _rel_err(r_mixed_sub[:, inside], tr.r_hist[:, inside], 0.5)
+        out["error_vs_fp64_inside"] = e_in
+    return {"metric": "particle-steps/s, mixed vs float64, and the mixed form's error (large-scale sector ring)",
+            "workload": "sector_ring_protons", "particles": wl.n, "steps": wl.nsteps, "dt": wl.dt,
+            "map": "512^3 float32 Bz over a 1 m cube (Bx = By = 0: the Bz-only record layout)",
+            "sort_every": args.sort_every, "map_bytes_mixed": dfm.map_bytes,
+            "error_metric": "per particle max over the start and end records of |r - r64| / max(|r64|, 0.5 m)",
+            "results": out}
 
 
 def run_serving(n_jobs, device, rate=50.0):
@@ -188,6 +317,11 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.workload != "rf_gap":
+        if rank == 0:
+            fn = run_pusher_sweep if args.workload == "pusher_sweep" else run_sector_ring
+            print(json.dumps(fn(args, dev)), flush=True)
+        return
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)

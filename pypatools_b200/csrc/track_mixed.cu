@@ -291,6 +291,21 @@ __device__ __forceinline__ void vel_add(float vh[3], float vl[3], F3 d) {
     ff_add(vh[2], vl[2], d.z);
 }
 
+// A Boris increment d, scaled by (1 + ws) into the float-float velocity.
+// hqdt = q/m dt/2 rounded to float32 carries one fixed relative error ws
+// (2.6e-8 for 5 MeV protons at dt = 1e-10 s) into a and t on every step: a
+// bias of the rotation angle that grows with the number of turns, where the
+// other roundings vary from step to step.  d (1 + ws) is exact for the 2a
+// part and for the rotation to first order (the neglected part is ~ t^2 of
+// the correction); d ws is below half an ulp of d, so it goes into the low
+// word, and costs three FMAs off the step's critical path.
+__device__ __forceinline__ void vel_add_boris(float vh[3], float vl[3], F3 d, float ws) {
+    vel_add(vh, vl, d);
+    vl[0] = fmaf(d.x, ws, vl[0]);
+    vl[1] = fmaf(d.y, ws, vl[1]);
+    vl[2] = fmaf(d.z, ws, vl[2]);
+}
+
 __device__ __forceinline__ void vel_set(float vh[3], float vl[3], F3 v) {
     // replace the state by a float32 value (clamped / recomputed velocity)
     vh[0] = v.x; vh[1] = v.y; vh[2] = v.z;
@@ -430,7 +445,8 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], f
         F3 E, B;
         if (fields_mixed<RF, L>(c, cell, fn, g, 0.0, E, B)) {
             F3 v = f3(vh[0], vh[1], vh[2]);
-            vel_add(vh, vl, ALG == PPT_ALG_BORIS ? boris_dv(v, E, B, P.hqdt) : P.dtf * lorentz_f(v, E, B, P.qm));
+            if constexpr (ALG == PPT_ALG_BORIS) vel_add_boris(vh, vl, boris_dv(v, E, B, P.hqdt), P.wscale);
+            else vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
             increment(P, vh, vl, d.dh, d.dl);
         }
         // where fields act (or may), the full float-float increment and a carry
@@ -543,7 +559,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 F3 E, B;
                 if (fields_mixed<RF, L>(c, cell, f, P.step0, 0.0, E, B))
                     // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
-                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt));
+                    vel_add_boris(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt), P.wscale);
             }
             if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
         }
@@ -611,7 +627,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 }
                 if (fields_mixed<RF, L>(c, cn, fn, P.nsteps_total, 0.0, E, B))
                     // Boris push with time step +dt/2 (pusher.py:993-1007)
-                    vel_add(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt));
+                    vel_add_boris(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt), P.wscale);
                 if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
             }
         }
@@ -792,12 +808,19 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
     P->wdt = a->rf_omega * a->dt;
     P->qm = (float)a->q_over_m;
     P->hqdt = (float)(0.5 * a->q_over_m * a->dt);
+    P->wscale = 0.0f;
+    if (st->algorithm == PPT_ALG_BORIS) {
+        // Boris increments scaled by (1 + wscale): hqdt (1 + wscale) is q/m
+        // dt/2 to float64 accuracy
+        const double exact = 0.5 * a->q_over_m * a->dt;
+        const double ws = exact / (double)P->hqdt - 1.0;
+        P->wscale = (float)ws;
+    }
     P->dtf = (float)a->dt;
     P->rf_phase = a->rf_phase;
     // the launch's per-step RF table covers steps step0 .. step0 + nsteps
     // (the closing half step reads the last one)
     P->rf_tab_n = (a->rf_phase && a->nsteps + 1 <= kRfTable) ? (int32_t)(a->nsteps + 1) : 0;
-    P->pad = 0;
     P->ci = st->i32;
     P->fs = st->f32;
     P->r_hist = a->r_hist;

@@ -46,7 +46,7 @@ struct TrackMixDev {
     double omega;
     double wdt;      // omega dt
     float qm;        // q/m
-    float hqdt;      // 0.5 q/m dt
+    float hqdt;      // 0.5 q/m dt, rounded to float32 (wscale below corrects the rounding)
     float dtf;       // dt
     float kh[3];     // dt / d: cell units per (m/s), as a float-float pair
     float kl[3];
@@ -61,7 +61,7 @@ struct TrackMixDev {
     int* status;
     unsigned long long* counters;
     int32_t rf_tab_n;   // entries of the per-step RF table a launch builds (0: none)
-    int32_t pad;
+    float wscale;       // Boris: (0.5 q/m dt) / hqdt - 1, applied to each velocity increment
 };
 
 // One (form, algorithm, RF) class of serving jobs: a block-level work queue
