@@ -61,8 +61,8 @@ def parse():
 
 # DRAM bytes per particle per launch of the mixed track kernel, from the ncu
 # capture of a 100-step in-map launch on the RF-gap workload at 1e6 protons
-# (the state read and written; the map's occupied cells stay in L2).
-MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 66.5
+# (the state read and written; the map's occupied cells stay in L1/L2).
+MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 65.7
 
 
 def _timed_track(tr, r0, v0, nsteps, sort_every, phase=None):
@@ -451,12 +451,13 @@ def main():
                                   "at 1e6 protons (profiles/track_mixed_kernel_rf_gap_1e6_in_map.txt), scaled "
                                   "by particle count; the gathers are served from L1/L2",
                 "peak_kind": f"{peak_kind} hbm_gbs",
-                "kernel": "track_mixed_kernel<BORIS,RF>", "avg_launch_ms": avg_launch_s * 1e3,
+                "kernel": "track_mixed_kernel<BORIS,RF,Ez|Bz layout>", "avg_launch_ms": avg_launch_s * 1e3,
                 "in_map_fraction": hits / max(1, m["counters"]["particle_steps"]),
-                "note": "algorithmic bytes as defined for this path count every corner gather, but the "
-                        "gathers of cell-sorted particles are served from L1 (96 % hit rate) and the DRAM "
-                        "traffic is the state in and out (traffic); frac above 1 says the kernel is not "
-                        "HBM-bound: ncu shows it issue-bound in the map (81 % issue-active)"}
+                "note": "algorithmic bytes as defined for this path count every corner gather of the "
+                        "stored components, but the gathers of cell-sorted particles are served from L1 "
+                        "and the DRAM traffic is the state in and out (traffic); the kernel is not "
+                        "HBM-bound: ncu shows it issue-bound in the map (87 % issue-active, 252 "
+                        "warp-instructions per warp-step)"}
 
     # e2e through the public API with host buffers (H2D of r0/v0/phase, D2H of the histories)
     e2e = None
