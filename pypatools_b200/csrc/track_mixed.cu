@@ -25,10 +25,9 @@ struct MixCtx {
     const TrackMixDev* P;
     double phase;            // omega t0 + phi_i
     unsigned hits;
-    double c0, s0;           // cos, sin of the phase
-    const double2* tab;      // (cos, sin) of g omega dt for g = tab0 .. tab0 + tab_n - 1, or NULL
-    int64_t tab0;
-    int tab_n;
+    float c0, s0;            // cos, sin of the phase
+    const float2* tab;       // (cos, sin) of g omega dt for every g of the launch, or NULL
+    int64_t tab0;            // the launch's first step
 };
 
 // Per-step RF table length limit: the sorted launches of a bunch crossing
@@ -42,30 +41,31 @@ __device__ __forceinline__ void rf_turn(int64_t g, double wdt, double& cg, doubl
 }
 
 // cos(omega (t0 + g dt) + phi_i) = cos(a + b) = cos a cos b - sin a sin b
-// with a = omega t0 + phi_i per particle and b = g omega dt per step, in
-// float64 and rounded once to float32.  The value depends on g and the
-// particle only (table or not), so tracks split into launches differently
-// agree bit for bit.
+// with a = omega t0 + phi_i per particle and b = g omega dt per step: both
+// angles' cosines and sines are formed in float64 and rounded to float32,
+// then combined by one float32 product and one FMA (within 1.4e-7 of the
+// cosine, rms 2.8e-8).  The value depends on g and the particle only, table
+// or not, so tracks split into launches differently agree bit for bit.  A
+// launch's table covers every step it evaluates (step0 .. step0 + nsteps).
 __device__ __forceinline__ float rf_cos(const MixCtx& c, int64_t g) {
-    double cg, sg;
-    const int64_t k = g - c.tab0;
-    if (c.tab != nullptr && k >= 0 && k < c.tab_n) {
-        const double2 t = c.tab[k];
-        cg = t.x;
-        sg = t.y;
+    float2 t;
+    if (c.tab != nullptr) {
+        t = c.tab[(int)(g - c.tab0)];
     } else {
+        double cg, sg;
         rf_turn(g, c.P->wdt, cg, sg);
+        t = make_float2((float)cg, (float)sg);
     }
-    return (float)fma(c.c0, cg, -(c.s0 * sg));
+    return fmaf(c.c0, t.x, -(c.s0 * t.y));
 }
 
 // Fill the block's RF table for steps step0 .. step0 + n - 1 (all threads
 // of the block call it; n <= kRfTable).
-__device__ __forceinline__ void build_rf_table(double2* tab, int64_t step0, int n, double wdt) {
+__device__ __forceinline__ void build_rf_table(float2* tab, int64_t step0, int n, double wdt) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         double cg, sg;
         rf_turn(step0 + i, wdt, cg, sg);
-        tab[i] = make_double2(cg, sg);
+        tab[i] = make_float2((float)cg, (float)sg);
     }
     __syncthreads();
 }
@@ -552,7 +552,10 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
         const int64_t row = P.order ? P.order[s] : s;
         if (RF) {
             c.phase = fma(P.omega, P.t0, P.rf_phase[s]);   // omega t0 + phi_i
-            sincos(c.phase, &c.s0, &c.c0);
+            double sa, ca;
+            sincos(c.phase, &sa, &ca);
+            c.c0 = (float)ca;
+            c.s0 = (float)sa;
         }
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
@@ -652,14 +655,13 @@ template <int ALG, bool RF, int L>
 __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u, 0.0, 0.0, nullptr, 0, 0};
+    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, nullptr, 0};
     if constexpr (RF) {
-        extern __shared__ double2 rf_tab[];
+        extern __shared__ float2 rf_tab[];
         if (P.rf_tab_n > 0) {
             build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
             c.tab = rf_tab;
             c.tab0 = P.step0;
-            c.tab_n = P.rf_tab_n;
         }
     }
     if (s < P.n) steps_done = track_mixed_particle<ALG, RF, L>(P, s, c);
@@ -697,16 +699,15 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
         __syncthreads();
         if (sP.flags >= 0) {
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
-            MixCtx c{&sP, 0.0, 0u, 0.0, 0.0, nullptr, 0, 0};
+            MixCtx c{&sP, 0.0, 0u, 0.0f, 0.0f, nullptr, 0};
             if constexpr (RF) {
                 // this job's step window, when the launch reserved a table for it
-                extern __shared__ double2 rf_tab[];
+                extern __shared__ float2 rf_tab[];
                 const int nt = (int)sP.nsteps + 1;
                 if (Q.chunk + 1 <= kRfTable && nt <= kRfTable) {
                     build_rf_table(rf_tab, sP.step0, nt, sP.wdt);
                     c.tab = rf_tab;
                     c.tab0 = sP.step0;
-                    c.tab_n = nt;
                 }
             }
             unsigned sd = 0;
@@ -726,11 +727,11 @@ static cudaError_t launch_mixed_layout(const TrackMixDev* P, const JobQueueDev* 
     if (P) {
         const int block = pick_block(P->n);
         const int g = grid_for(P->n, block);
-        const size_t smem = (size_t)P->rf_tab_n * sizeof(double2);
+        const size_t smem = (size_t)P->rf_tab_n * sizeof(float2);
         if (rf && kE) track_mixed_kernel<ALG, kE, L><<<g, block, smem, s>>>(*P);
         else track_mixed_kernel<ALG, false, L><<<g, block, 0, s>>>(*P);
     } else {
-        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(double2) : 0;
+        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(float2) : 0;
         if (rf && kE) track_mixed_jobs_kernel<ALG, kE, L><<<grid, kJobBlock, smem, s>>>(*Q);
         else track_mixed_jobs_kernel<ALG, false, L><<<grid, kJobBlock, 0, s>>>(*Q);
     }
