@@ -306,6 +306,34 @@ __device__ __forceinline__ void vel_add_boris(float vh[3], float vl[3], F3 d, fl
     vl[2] = fmaf(d.z, ws, vl[2]);
 }
 
+// The same for the Boris steps of a track, at a third of the cost: a fast
+// two-sum (exact when |vh| >= |d|, which holds but for a component passing
+// through zero, where its error stays below an ulp of d) whose rounding
+// error, and the correction d ws, go into the low word without renormalising
+// the pair.  vel_renorm renormalises it after global steps g with
+// (g + 1) % 4 == 0 that see a field, so the low word stays within a few ulps
+// of the high one and a track's bits do not depend on how it is split into
+// launches.  vh + vl stays the accumulated velocity throughout.
+__device__ __forceinline__ void vel_add_fast(float vh[3], float vl[3], F3 d, float ws) {
+    const float dd[3] = {d.x, d.y, d.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float s = vh[a] + dd[a];
+        const float err = dd[a] - (s - vh[a]);
+        vl[a] = fmaf(dd[a], ws, vl[a] + err);
+        vh[a] = s;
+    }
+}
+
+__device__ __forceinline__ void vel_renorm(float vh[3], float vl[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float s = vh[a] + vl[a];
+        vl[a] = vl[a] - (s - vh[a]);
+        vh[a] = s;
+    }
+}
+
 __device__ __forceinline__ void vel_set(float vh[3], float vl[3], F3 v) {
     // replace the state by a float32 value (clamped / recomputed velocity)
     vh[0] = v.x; vh[1] = v.y; vh[2] = v.z;
@@ -445,8 +473,12 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], f
         F3 E, B;
         if (fields_mixed<RF, L>(c, cell, fn, g, 0.0, E, B)) {
             F3 v = f3(vh[0], vh[1], vh[2]);
-            if constexpr (ALG == PPT_ALG_BORIS) vel_add_boris(vh, vl, boris_dv(v, E, B, P.hqdt), P.wscale);
-            else vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
+            if constexpr (ALG == PPT_ALG_BORIS) {
+                vel_add_fast(vh, vl, boris_dv(v, E, B, P.hqdt), P.wscale);
+                if (((unsigned)(g + 1) & 3u) == 0u) vel_renorm(vh, vl);
+            } else {
+                vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
+            }
             increment(P, vh, vl, d.dh, d.dl);
         }
         // where fields act (or may), the full float-float increment and a carry
