@@ -220,6 +220,7 @@ extern "C" int ppt_fieldmap_create_masked(const ppt_grid_desc* grid, uint32_t co
     m.dev.dtype = store_dtype;
     m.dev.sy = m.n[2];
     m.dev.sx = m.n[1] * m.n[2];
+    m.dev.idx32 = total_nodes * m.dev.stride < (1LL << 31) ? 1 : 0;
     size_t elem = store_dtype == PPT_DTYPE_F64 ? 8 : 4;
     m.bytes = (size_t)total_nodes * m.dev.stride * elem;
     PPT_CUDA_TRY(cudaGetDevice(&m.device));

@@ -75,6 +75,7 @@ struct MapDev {
     int b_off;        // element offset of B in a full-layout record (4)
     int dtype;        // PPT_DTYPE_F64 / PPT_DTYPE_F32
     int all_uniform;
+    int idx32;        // every element offset (nodes x stride) fits in int32
     AxisDev ax[3];
 };
 

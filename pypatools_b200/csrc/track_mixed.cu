@@ -113,13 +113,24 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     const float ux = 1.0f - tx, uy = 1.0f - ty, uz = 1.0f - tz;
     const float a00 = ux * uy, a01 = ux * ty, a10 = tx * uy, a11 = tx * ty;
     const float w[8] = {a00 * uz, a00 * tz, a01 * uz, a01 * tz, a10 * uz, a10 * tz, a11 * uz, a11 * tz};
-    const int64_t node = (int64_t)i * m.sx + (int64_t)j * m.sy + k;
     constexpr int W = layout_width(L);
-    // corner (di, dj) = (0,0) (0,1) (1,0) (1,1); the k+1 corner is the next record
-    const float* p00 = static_cast<const float*>(m.data) + node * W;
-    const float* p10 = p00 + m.sx * W;
-    const float* p01 = p00 + m.sy * W;
-    const float* p11 = p10 + m.sy * W;
+    // corner (di, dj) = (0,0) (0,1) (1,0) (1,1); the k+1 corner is the next
+    // record; 32-bit offsets when the map's elements allow (maps below 2^31)
+    const float* p00;
+    const float* p10;
+    const float* p01;
+    if (m.idx32) {
+        const int sx = (int)m.sx * W, sy = (int)m.sy * W;
+        p00 = static_cast<const float*>(m.data) + (i * sx + j * sy + k * W);
+        p10 = p00 + sx;
+        p01 = p00 + sy;
+    } else {
+        const int64_t node = (int64_t)i * m.sx + (int64_t)j * m.sy + k;
+        p00 = static_cast<const float*>(m.data) + node * W;
+        p10 = p00 + m.sx * W;
+        p01 = p00 + m.sy * W;
+    }
+    const float* p11 = p01 + (p10 - p00);
     const float* pc[4] = {p00, p01, p10, p11};
     if constexpr (L == kLayFull) {
         // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner
