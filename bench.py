@@ -186,6 +186,57 @@ def run_sector_ring(args, dev):
             "results": out}
 
 
+def run_deposit(r, dev, mesh_extent=(0.02, 0.02, 0.3), mesh_cells=(32, 32, 128), reps=5):
+    """Cloud-in-cell deposition of the bunch (positions r, (n,3) CUDA float64,
+    unit charges) onto a space-charge mesh around it, in the given particle order
+    and sorted by mesh cell; device time per deposit (best of reps), the bytes
+    it must move at HBM bandwidth, and the NumPy oracle on a 1e6 sample."""
+    import torch
+    from pypatools_b200 import _lib
+    from oracle.deposit_oracle import bin_particles_cic as oracle_cic
+    lib = _lib.load()
+    n = r.shape[0]
+    q = torch.full((n,), 1.602176634e-19, dtype=torch.float64, device=dev)
+    mesh = _lib.MeshDesc()
+    for a in range(3):
+        mesh.extent[a] = mesh_extent[a]
+        mesh.cells[a] = mesh_cells[a]
+    nodes = mesh_cells[0] * mesh_cells[1] * mesh_cells[2]
+    rho = torch.empty(nodes, dtype=torch.float64, device=dev)
+    h = torch.tensor([e / c for e, c in zip(mesh_extent, mesh_cells)], dtype=torch.float64, device=dev)
+    key = torch.floor((r + torch.tensor(mesh_extent, dtype=torch.float64, device=dev) / 2) / h).to(torch.int64)
+    key = key.clamp(min=0)
+    lin = (key[:, 0] * mesh_cells[1] + key[:, 1]) * mesh_cells[2] + key[:, 2]
+    r_sorted = r[torch.argsort(lin)].contiguous()
+    out = {}
+    for name, rr in (("given_order", r), ("cell_sorted", r_sorted)):
+        best = None
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            _lib.check(lib.ppt_deposit_cic(n, rr.data_ptr(), q.data_ptr(), mesh, rho.data_ptr(),
+                                           _lib.stream_handle()))
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b)
+            best = ms if best is None or ms < best else best
+        out[name] = {"ms": best, "particles_per_s": n / (best / 1e3)}
+    peak, peak_kind = measured_peaks()
+    alg_bytes = n * 32 + 3 * nodes * 8       # positions + charges in; rho zeroed, written, divided
+    ms = out["cell_sorted"]["ms"]
+    out["roofline"] = {"bound": "hbm", "achieved": alg_bytes / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                       "frac": alg_bytes / (ms / 1e3) / 1e9 / peak, "peak_kind": f"{peak_kind} hbm_gbs"}
+    sample = min(n, 1_000_000)
+    rs = r[:sample].cpu().numpy()
+    qs = np.full(sample, 1.602176634e-19)
+    t = time.perf_counter()
+    oracle_cic(rs, qs, mesh_extent, mesh_cells)
+    out["cpu_oracle_particles_per_s"] = sample / (time.perf_counter() - t)
+    out["mesh"] = f"{mesh_cells[0]}x{mesh_cells[1]}x{mesh_cells[2]} nodes over {mesh_extent} m"
+    out["particles"] = n
+    return out
+
+
 def run_serving(n_jobs, device, rate=50.0):
     """The serving stream (Poisson arrivals at 50 jobs/s, 1e3-1e6 protons,
     Boris / Vay / RK4, 1000-10000 steps, 4 resident float32 maps 64^3-256^3,
@@ -483,6 +534,10 @@ def main():
                "api": "PusherGPU.track_batch (numpy in, numpy histories out)", "steps": args.e2e_steps}
         del rh, vh
 
+    deposit = None
+    if rank == 0:
+        deposit = run_deposit(d_r0, dev)
+
     serving = None
     if args.serve_jobs > 0:
         torch.cuda.empty_cache()
@@ -517,6 +572,7 @@ def main():
             "gpu_launches": m["launches"],
             "clocks": clocks,
             "serving": serving,
+            "deposit": deposit,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

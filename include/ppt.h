@@ -24,6 +24,8 @@
  *                   (pusher.py:934-962, :1012)
  *   ppt_moments     ParticleDistribution statistics (src/PyPATools/particles.py:
  *                   693-719, :761-788, :507-525, :393-457)
+ *   ppt_deposit_cic PyAMGPoissonSolver's CIC charge deposition
+ *                   (src/PyPATools/poisson_amg.py:849-911)
  *   ppt_cell_sort   no reference counterpart: particle reordering for gather
  *                   locality (the reference has no particle ordering step)
  */
@@ -255,6 +257,25 @@ int ppt_jobs_destroy(ppt_jobs* jobs);
 int64_t ppt_cell_sort_scratch_bytes(int64_t n);
 int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* order, double* rf_phase,
                   void* scratch, void* stream);
+
+/* Poisson mesh of the reference's space-charge solver: cells[d] nodes per
+ * axis spaced extent[d] / cells[d], the first at -extent[d] / 2 (the
+ * reference's domain_extent and mesh_cells). */
+typedef struct {
+    double extent[3];
+    int64_t cells[3];
+} ppt_mesh_desc;
+
+/* Cloud-in-cell charge deposition (PyAMGPoissonSolver._bin_particles_cic_cpu
+ * and _cic_deposit_numba, src/PyPATools/poisson_amg.py:849-911): rho (device
+ * float64, cells[0]*cells[1]*cells[2], [i][j][k] with k fastest) is
+ * overwritten with the charge per cell volume of the n particles at r
+ * (device (n,3) float64) with charges q (device float64 [n]).  Positions are
+ * clamped onto the mesh as the reference does (a particle on or beyond the
+ * last node lands on the node before it); a NaN position deposits nothing.
+ * Float64 atomics: results agree with the sequential sum to rounding. */
+int ppt_deposit_cic(int64_t n, const double* r, const double* q, const ppt_mesh_desc* mesh, double* rho,
+                    void* stream);
 
 /* Bunch moments of n particles from (n,3) float64 positions and velocities
  * (device), in float64:

@@ -13,7 +13,8 @@ from .field import Field, ScaledField, CompositeField, FieldMap, get_interpolato
 from .pusher import Pusher, PusherGPU, RFModulation, DeviceTracker
 from .particles import ParticleDistribution
 from .moments import bunch_moments
+from .deposit import bin_particles_cic
 
 __all__ = ["IonSpecies", "PRESETS", "Field", "ScaledField", "CompositeField", "FieldMap", "get_interpolator",
            "CudaInterpolator", "Pusher", "PusherGPU", "RFModulation", "DeviceTracker", "ParticleDistribution",
-           "bunch_moments"]
+           "bunch_moments", "bin_particles_cic"]

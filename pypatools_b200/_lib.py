@@ -67,9 +67,14 @@ class JobDesc(ctypes.Structure):
 
 
 # name -> (restype, argtypes); every symbol include/ppt.h declares
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("extent", c_double * 3), ("cells", c_int64 * 3)]
+
+
 SIGNATURES = {
     "ppt_fieldmap_create": (c_int, [POINTER(GridDesc), c_int, c_int, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_layout": (c_int, [c_uint32]),
+    "ppt_deposit_cic": (c_int, [c_int64, c_void_p, c_void_p, POINTER(MeshDesc), c_void_p, c_void_p]),
     "ppt_fieldmap_create_masked": (c_int, [POINTER(GridDesc), c_uint32, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_add": (c_int, [c_void_p, POINTER(c_void_p * 6), POINTER(c_double * 6), c_int, c_void_p]),
     "ppt_fieldmap_destroy": (c_int, [c_void_p]),

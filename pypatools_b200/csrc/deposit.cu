@@ -1,0 +1,141 @@
+// Cloud-in-cell charge deposition onto a Poisson mesh: the particle -> grid
+// step that feeds a space-charge solve, next to the push.
+//
+// Reference: PyAMGPoissonSolver._bin_particles_cic_cpu and its kernel
+// _cic_deposit_numba (src/PyPATools/poisson_amg.py:849-911).  The mesh has
+// cells[d] nodes per axis, spaced h = extent / cells from -extent / 2
+// (:178-185); rho is indexed [i][j][k], k fastest.  Per particle, in float64
+// as there:
+//   p = clip((x + extent/2) / h, 0, cells - 1)      (position in node units)
+//   i = floor(p);  f = p - i;  i = clip(i, 0, cells - 2)
+//   rho[corner] += q * wx * wy * wz  over the 8 corners, w = 1 - f or f
+// and finally rho /= hx hy hz.  Because f is taken before i is clipped, a
+// particle at p = cells - 1 (exactly on the last node, or clamped onto it from
+// beyond) puts all its charge on the node before the last; that is kept.
+//
+// One thread per particle, float64 atomics into rho.  A cell-sorted bunch
+// puts whole warps into one cell: then the warp sums each corner's value with
+// shuffles first and issues 8 atomics instead of 256.  The summation order
+// differs from the reference's sequential loop, so results agree to rounding.
+// A particle with a NaN coordinate deposits nothing (the reference's cast of
+// NaN to an index is undefined).
+#include <cmath>
+
+#include "ppt_internal.cuh"
+
+namespace ppt {
+
+struct MeshGeom {
+    double half[3];   // extent / 2
+    double h[3];      // extent / cells
+    int64_t n[3];     // nodes per axis (the reference's mesh_cells)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void deposit_cic_kernel(int64_t n, const double* __restrict__ r, const double* __restrict__ q,
+                                   MeshGeom G, double* __restrict__ rho) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    bool valid = s < n;
+    int64_t base = -1;
+    double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t strides[3] = {G.n[1] * G.n[2], G.n[2], 1};
+    if (valid) {
+        int64_t idx[3];
+        double f[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            double p = (r[3 * s + a] + G.half[a]) / G.h[a];
+            valid = valid && !isnan(p);                        // a NaN position deposits nothing
+            const double top = (double)(G.n[a] - 1);
+            p = p < 0.0 ? 0.0 : (p > top ? top : p);          // np.clip
+            p = isnan(p) ? 0.0 : p;
+            double i = floor(p);
+            f[a] = p - i;
+            const double itop = (double)(G.n[a] - 2);
+            i = i < 0.0 ? 0.0 : (i > itop ? itop : i);
+            idx[a] = (int64_t)i;
+        }
+        base = idx[0] * strides[0] + idx[1] * strides[1] + idx[2];
+        const double qs = q[s];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
+            const double wx = di ? f[0] : 1.0 - f[0];
+            const double wy = dj ? f[1] : 1.0 - f[1];
+            const double wz = dk ? f[2] : 1.0 - f[2];
+            w[c] = qs * (wx * wy * wz);
+        }
+    }
+    // An invalid lane (past n, or a NaN position) gets key -1 and no charge,
+    // so a warp whose 32 keys agree either is all valid and in one cell (it
+    // sums with full-mask shuffles, all 32 lanes taking part) or is all invalid.
+    if (!valid) {
+        base = -1;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) w[c] = 0.0;
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)base);
+    if (peers == 0xffffffffu && valid) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) w[c] = warp_sum(w[c]);
+        if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
+                atomicAdd(rho + base + di * strides[0] + dj * strides[1] + dk, w[c]);
+            }
+        }
+        return;
+    }
+    if (!valid) return;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
+        atomicAdd(rho + base + di * strides[0] + dj * strides[1] + dk, w[c]);
+    }
+}
+
+__global__ void mesh_divide_kernel(int64_t m, double* __restrict__ rho, double volume) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+        rho[i] = rho[i] / volume;
+}
+
+}  // namespace ppt
+
+using namespace ppt;
+
+extern "C" int ppt_deposit_cic(int64_t n, const double* r, const double* q, const ppt_mesh_desc* mesh, double* rho,
+                               void* stream) {
+    if (!mesh || !rho) return fail(PPT_ERR_ARG, "mesh and rho must not be NULL");
+    if (n < 0) return fail(PPT_ERR_ARG, "n must be >= 0");
+    if (n > 0 && (!r || !q)) return fail(PPT_ERR_ARG, "r and q must not be NULL");
+    MeshGeom G;
+    int64_t nodes = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (mesh->cells[a] < 2) return fail(PPT_ERR_ARG, "every mesh axis needs at least 2 nodes");
+        if (!(mesh->extent[a] > 0.0)) return fail(PPT_ERR_ARG, "mesh extents must be positive");
+        G.n[a] = mesh->cells[a];
+        G.half[a] = mesh->extent[a] / 2.0;
+        G.h[a] = mesh->extent[a] / (double)mesh->cells[a];
+        nodes *= mesh->cells[a];
+        if (nodes > (1LL << 40)) return fail(PPT_ERR_ARG, "mesh too large");
+    }
+    const double volume = G.h[0] * G.h[1] * G.h[2];
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    PPT_CUDA_TRY(cudaMemsetAsync(rho, 0, (size_t)nodes * sizeof(double), s));
+    if (n > 0) {
+        const int block = 256;
+        deposit_cic_kernel<<<grid_for(n, block), block, 0, s>>>(n, r, q, G, rho);
+        PPT_CUDA_TRY(cudaGetLastError());
+    }
+    const int block = 256;
+    int64_t g = (nodes + block - 1) / block;
+    mesh_divide_kernel<<<(int)(g > 148 * 16 ? 148 * 16 : g), block, 0, s>>>(nodes, rho, volume);
+    PPT_CUDA_TRY(cudaGetLastError());
+    return PPT_OK;
+}
