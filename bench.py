@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--long-chunk", type=int, default=1000,
                     help="steps per launch once the bunch has left the map (no sorts then)")
-    ap.add_argument("--sort-every", type=int, default=100,
-                    help="cell re-sort interval in steps (also the launch length); 0 = never")
+    ap.add_argument("--sort-every", type=int, default=None,
+                    help="cell re-sort interval in steps while the map is populated (also the launch length "
+                         "then); 0 = never; default 300 for rf_gap (best of a 50-1000 sweep), 100 otherwise "
+                         "(the sector-ring configuration's interval)")
     ap.add_argument("--serve-jobs", type=int, default=300,
                     help="jobs of the serving stream per form (2000 = the full stream); 0 skips it")
     args = ap.parse_args()
@@ -56,6 +58,8 @@ def parse():
                 "sector_ring": (100_000_000, 50_000)}[args.workload]
     args.n = args.n or defaults[0]
     args.nsteps = args.nsteps or defaults[1]
+    if args.sort_every is None:
+        args.sort_every = 300 if args.workload == "rf_gap" else 100
     return args
 
 
