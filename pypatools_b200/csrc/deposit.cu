@@ -13,10 +13,9 @@
 // particle at p = cells - 1 (exactly on the last node, or clamped onto it from
 // beyond) puts all its charge on the node before the last; that is kept.
 //
-// One thread per particle, float64 atomics into rho.  A cell-sorted bunch
-// puts whole warps into one cell: then the warp sums each corner's value with
-// shuffles first and issues 8 atomics instead of 256.  The summation order
-// differs from the reference's sequential loop, so results agree to rounding.
+// Float64 atomics into rho; for a cell-sorted bunch, warps keep running sums
+// per cell (deposit_cic_kernel below).  The summation order differs from the
+// reference's sequential loop, so results agree to rounding.
 // A particle with a NaN coordinate deposits nothing (the reference's cast of
 // NaN to an index is undefined).
 #include <cmath>
@@ -37,16 +36,15 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-__global__ void deposit_cic_kernel(int64_t n, const double* __restrict__ r, const double* __restrict__ q,
-                                   MeshGeom G, double* __restrict__ rho) {
-    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// One particle's cell (linear index of its lower corner) and corner charges;
+// an invalid particle (past n, or a NaN position) gets cell -1 and no charge.
+__device__ __forceinline__ int64_t particle_corners(int64_t s, int64_t n, const double* __restrict__ r,
+                                                    const double* __restrict__ q, const MeshGeom& G,
+                                                    const int64_t strides[3], double w[8]) {
     bool valid = s < n;
-    int64_t base = -1;
-    double w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t strides[3] = {G.n[1] * G.n[2], G.n[2], 1};
+    int64_t idx[3] = {0, 0, 0};
+    double f[3] = {0.0, 0.0, 0.0};
     if (valid) {
-        int64_t idx[3];
-        double f[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             double p = (r[3 * s + a] + G.half[a]) / G.h[a];
@@ -60,43 +58,77 @@ __global__ void deposit_cic_kernel(int64_t n, const double* __restrict__ r, cons
             i = i < 0.0 ? 0.0 : (i > itop ? itop : i);
             idx[a] = (int64_t)i;
         }
-        base = idx[0] * strides[0] + idx[1] * strides[1] + idx[2];
-        const double qs = q[s];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
-            const double wx = di ? f[0] : 1.0 - f[0];
-            const double wy = dj ? f[1] : 1.0 - f[1];
-            const double wz = dk ? f[2] : 1.0 - f[2];
-            w[c] = qs * (wx * wy * wz);
-        }
     }
-    // An invalid lane (past n, or a NaN position) gets key -1 and no charge,
-    // so a warp whose 32 keys agree either is all valid and in one cell (it
-    // sums with full-mask shuffles, all 32 lanes taking part) or is all invalid.
-    if (!valid) {
-        base = -1;
+    const double qs = valid ? q[s] : 0.0;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) w[c] = 0.0;
+    for (int c = 0; c < 8; ++c) {
+        const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
+        const double wx = di ? f[0] : 1.0 - f[0];
+        const double wy = dj ? f[1] : 1.0 - f[1];
+        const double wz = dk ? f[2] : 1.0 - f[2];
+        w[c] = valid ? qs * (wx * wy * wz) : 0.0;
     }
-    const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)base);
-    if (peers == 0xffffffffu && valid) {
-#pragma unroll
-        for (int c = 0; c < 8; ++c) w[c] = warp_sum(w[c]);
-        if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
-                atomicAdd(rho + base + di * strides[0] + dj * strides[1] + dk, w[c]);
-            }
-        }
-        return;
-    }
-    if (!valid) return;
+    return valid ? idx[0] * strides[0] + idx[1] * strides[1] + idx[2] : -1;
+}
+
+__device__ __forceinline__ void add_corners(double* rho, int64_t base, const int64_t strides[3], const double w[8]) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
         atomicAdd(rho + base + di * strides[0] + dj * strides[1] + dk, w[c]);
+    }
+}
+
+// Each warp takes kRounds rounds of 32 consecutive particles.  While all 32
+// particles of a round are valid and in the same cell as the warp's running
+// sums, each lane just adds its corner charges to its own running sums; when
+// the cell changes (or at the end) the warp reduces them with shuffles and
+// lane 0 issues 8 atomics.  A round whose particles are not all in one cell
+// adds per lane.  A cell-sorted bunch thus costs 8 atomics per cell and warp
+// instead of 8 per particle.
+constexpr int kRounds = 8;
+
+__global__ void __launch_bounds__(256) deposit_cic_kernel(int64_t n, const double* __restrict__ r,
+                                                          const double* __restrict__ q, MeshGeom G,
+                                                          double* __restrict__ rho) {
+    const int64_t strides[3] = {G.n[1] * G.n[2], G.n[2], 1};
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t first = warp * (32 * kRounds);
+    int64_t cur = -1;                 // cell of the running sums (warp-uniform), -1: none
+    double acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+    for (int round = 0; round < kRounds; ++round) {
+        const int64_t s = first + round * 32 + lane;
+        if (first + round * 32 >= n) break;          // warp-uniform
+        double w[8];
+        const int64_t base = particle_corners(s, n, r, q, G, strides, w);
+        const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)base);
+        const bool uniform = peers == 0xffffffffu && base >= 0;   // the same for every lane
+        if (uniform && base == cur) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[c] += w[c];
+            continue;
+        }
+        if (cur >= 0) {                               // flush the running sums
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[c] = warp_sum(acc[c]);
+            if (lane == 0) add_corners(rho, cur, strides, acc);
+            cur = -1;
+        }
+        if (uniform) {
+            cur = base;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc[c] = w[c];
+        } else if (base >= 0) {
+            add_corners(rho, base, strides, w);
+        }
+    }
+    if (cur >= 0) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] = warp_sum(acc[c]);
+        if (lane == 0) add_corners(rho, cur, strides, acc);
     }
 }
 
@@ -130,7 +162,8 @@ extern "C" int ppt_deposit_cic(int64_t n, const double* r, const double* q, cons
     PPT_CUDA_TRY(cudaMemsetAsync(rho, 0, (size_t)nodes * sizeof(double), s));
     if (n > 0) {
         const int block = 256;
-        deposit_cic_kernel<<<grid_for(n, block), block, 0, s>>>(n, r, q, G, rho);
+        const int64_t per_block = (int64_t)block * kRounds;
+        deposit_cic_kernel<<<(int)((n + per_block - 1) / per_block), block, 0, s>>>(n, r, q, G, rho);
         PPT_CUDA_TRY(cudaGetLastError());
     }
     const int block = 256;
