@@ -15,7 +15,8 @@ return shapes and error messages:
 and adds keyword-only options: ``precision`` ('fp64' = the reference method
 in float64, the drop-in; 'mixed' = the mixed-precision form), ``device``,
 ``snapshot`` ('host' numpy arrays like the reference, or 'device' torch
-tensors), ``steps_per_launch``, ``sort_every`` (cell re-sort interval) and,
+tensors), ``steps_per_launch``, ``sort_every`` (cell re-sort interval; 'auto' = every 300
+steps for bunches of 65536 or more, none below) and,
 on ``track_batch``, ``rf`` (an ``RFModulation`` multiplying E by
 cos(2 pi f t + phi_i)) and ``t0``.
 
@@ -290,7 +291,7 @@ class PusherGPU:
     EXTRA_ALGORITHMS = list(EXTRA_ALGORITHMS)
 
     def __init__(self, ion, algorithm="boris", use_numba=True, electrode_assembly=None, *, precision="fp64",
-                 device=None, snapshot="host", steps_per_launch=None, sort_every=0):
+                 device=None, snapshot="host", steps_per_launch=None, sort_every="auto"):
         self.ion = ion
         self.q_over_m = ion.q_over_m
         algorithm = algorithm.lower()
@@ -316,11 +317,25 @@ class PusherGPU:
         self.device = device
         self.snapshot = snapshot
         self.steps_per_launch = steps_per_launch
-        self.sort_every = int(sort_every)
+        if sort_every != "auto":
+            sort_every = int(sort_every)
+        self.sort_every = sort_every
         self._fields = FieldCache(capacity=4)
         self.last_tracker = None
 
     # -- helpers -----------------------------------------------------------
+    # 'auto' cell-sort interval: bunches this large re-sort every AUTO_SORT_STEPS
+    # steps while they are in a map (sorting never changes a result, it only
+    # makes the corner gathers of a warp hit the same records); smaller bunches
+    # are not sorted, a sort costing more than it saves there.
+    AUTO_SORT_MIN_PARTICLES = 65536
+    AUTO_SORT_STEPS = 300
+
+    def _sort_interval(self, m):
+        if self.sort_every == "auto":
+            return self.AUTO_SORT_STEPS if m >= self.AUTO_SORT_MIN_PARTICLES else 0
+        return self.sort_every
+
     def _device_fields(self, efield, bfield):
         _torch()
         return self._fields.get(efield, bfield, self.precision, self.device)
@@ -399,8 +414,9 @@ class PusherGPU:
                            rf_omega=rf_omega, rf_phase=rf_phase, t0=t0, record=True, device=self.device)
         self.last_tracker = tr
         chunk = self.steps_per_launch or default_steps_per_launch(m, nsteps)
-        if self.sort_every > 0:
-            chunk = min(chunk, self.sort_every)
+        sort_every = self._sort_interval(m)
+        if sort_every > 0:
+            chunk = min(chunk, sort_every)
         to_host = self.snapshot == "host"
         with torch.cuda.device(df.device):
             if to_host:
@@ -434,7 +450,7 @@ class PusherGPU:
                     # the closing half step of the Boris family
                     drain(min(done // rec + 1, n_rec - 1))
 
-            tr.run(nsteps, chunk, sort_every=self.sort_every, after_launch=after_launch)
+            tr.run(nsteps, chunk, sort_every=sort_every, after_launch=after_launch)
             if to_host:
                 drain(n_rec)
                 copy_stream.synchronize()
