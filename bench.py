@@ -241,6 +241,56 @@ def run_deposit(r, dev, mesh_extent=(0.02, 0.02, 0.3), mesh_cells=(32, 32, 128),
     return out
 
 
+def run_electrodes(dev, n=1_000_000, nsteps=1000, reps=3):
+    """Electrode collision termination (float64 Boris): the quadrupole-solenoid
+    bunch through an aperture plate (5 mm hole) at z = 3 cm inside a 12 mm beam
+    pipe (2.4e3 triangles); device time of one 1000-step launch with and
+    without the surface, and the oracle's rate on a small sample."""
+    import torch
+    from pypatools_b200 import ElectrodeSurface, Field, workloads
+    from pypatools_b200.device_fields import DeviceFields
+    from pypatools_b200.pusher import DeviceTracker
+    from oracle import pusher_oracle as orc
+    wl = workloads.quad_solenoid_protons(n=n, nsteps=nsteps, rec_every=nsteps)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    df = DeviceFields(Field.zero(3), Field.from_arrays(g, wl.b_values), "fp64", dev)
+    surf = ElectrodeSurface.aperture_plate(0.03, 0.005, 0.02, n_phi=48, n_r=3) + \
+        ElectrodeSurface.tube(0.012, -0.05, 0.06, n_phi=48, n_z=22)
+    r0 = torch.from_numpy(wl.r0).to(dev)
+    v0 = torch.from_numpy(wl.v0).to(dev)
+    out = {}
+    stopped = None
+    for name, sf in (("without_surface", None), ("with_surface", surf)):
+        best = None
+        for _ in range(reps):
+            tr = DeviceTracker("boris", wl.species.q_over_m, df, n, nsteps, wl.dt, nsteps, "fp64", device=dev,
+                               surface=sf)
+            tr.load(r0, v0)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            tr.advance(nsteps)
+            b.record()
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b)
+            best = ms if best is None or ms < best else best
+            if sf is not None:
+                stopped = int(n - tr.active.sum().item())
+            del tr
+        out[name] = {"ms": best, "particle_steps_per_s": n * nsteps / (best / 1e3)}
+    out["overhead"] = out["with_surface"]["ms"] / out["without_surface"]["ms"]
+    out["stopped_fraction"] = stopped / n
+    out["triangles"] = int(surf.triangles.shape[0])
+    out["cells"] = surf.info(dev)["cells"]
+    sample, steps = 500, 40
+    e, bo = orc.ZeroField(), orc.MapField(wl.grid, wl.b_values)
+    t = time.perf_counter()
+    orc.track_batch("boris", wl.species.q_over_m, wl.r0[:sample], wl.v0[:sample], e, bo, steps, wl.dt, steps,
+                    surface=(surf.vertices, surf.triangles))
+    out["cpu_oracle_particle_steps_per_s"] = sample * steps / (time.perf_counter() - t)
+    out["workload"] = f"quad_solenoid_protons n={n}, {nsteps} steps, float64 boris, one launch"
+    return out
+
+
 def run_serving(n_jobs, device, rate=50.0):
     """The serving stream (Poisson arrivals at 50 jobs/s, 1e3-1e6 protons,
     Boris / Vay / RK4, 1000-10000 steps, 4 resident float32 maps 64^3-256^3,
@@ -538,9 +588,10 @@ def main():
                "api": "PusherGPU.track_batch (numpy in, numpy histories out)", "steps": args.e2e_steps}
         del rh, vh
 
-    deposit = None
+    deposit = electrodes = None
     if rank == 0:
         deposit = run_deposit(d_r0, dev)
+        electrodes = run_electrodes(dev)
 
     serving = None
     if args.serve_jobs > 0:
@@ -577,6 +628,7 @@ def main():
             "clocks": clocks,
             "serving": serving,
             "deposit": deposit,
+            "electrodes": electrodes,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

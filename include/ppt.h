@@ -26,6 +26,9 @@
  *                   693-719, :761-788, :507-525, :393-457)
  *   ppt_deposit_cic PyAMGPoissonSolver's CIC charge deposition
  *                   (src/PyPATools/poisson_amg.py:849-911)
+ *   ppt_surface_*   PyElectrodeAssembly.segment_intersects_surface, the collision
+ *                   test track_batch makes each step (pusher.py:982-990; the
+ *                   assembly comes from the external py_electrodes package)
  *   ppt_cell_sort   no reference counterpart: particle reordering for gather
  *                   locality (the reference has no particle ordering step)
  */
@@ -39,7 +42,7 @@
 extern "C" {
 #endif
 
-#define PPT_ABI_VERSION 1
+#define PPT_ABI_VERSION 2
 
 /* status codes */
 #define PPT_OK               0
@@ -90,7 +93,12 @@ typedef struct ppt_fieldmap ppt_fieldmap;   /* opaque */
 
 /* Node grid of one map: n[d] >= 2 sorted node coordinates per axis, given
  * as HOST arrays (copied).  Node values are indexed [i][j][k] with k
- * fastest, the 'ij' meshgrid order NumbaInterpolator uses. */
+ * fastest, the 'ij' meshgrid order NumbaInterpolator uses.
+ * n[d] == 1 (axis[d] is then ignored and may be NULL): the map does not vary
+ * along axis d and has no bounds on it -- the reference's 1D fields
+ * (n = {1, 1, nz}, values along z) and 2D fields (n = {nx, ny, 1}), which
+ * Field._get_field_1d / _get_field_2d evaluate at z and at (x, y)
+ * (src/PyPATools/field.py:457-489).  At least one axis needs 2 nodes. */
 typedef struct {
     int64_t n[3];
     const double* axis[3];
@@ -201,12 +209,40 @@ typedef struct {
     const int64_t* order; /* slot -> row (after ppt_cell_sort), NULL = identity */
     int32_t* status;      /* device int32, OR-ed with PPT_STATUS_* bits, or NULL */
     unsigned long long* counters; /* device u64[2]: +in-map gathers, +particle steps; or NULL */
+    const struct ppt_surface* surface; /* electrode surface (float64 form), or NULL: see below */
+    uint8_t* active;      /* with a surface: device uint8[n] in ROW order, 1 = still tracked */
 } ppt_track_args;
 
 /* Advance every particle nsteps steps in ONE kernel launch, state kept in
  * registers, fields gathered on the fly, snapshots written into r_hist /
- * v_hist at the reference's record indices. */
+ * v_hist at the reference's record indices.
+ * With args->surface (float64 form only; PPT_ERR_UNSUPPORTED otherwise) each
+ * step's segment (position before -> after the step) of every active particle
+ * is tested against the surface after the step's snapshot, and a particle
+ * that hits is stopped: active[row] = 0, its state stays at the step's end,
+ * later snapshots and the final half step leave its rows untouched
+ * (pusher.py:966-1007).  Set active to 1 before the first call. */
 int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_track_args* args, void* stream);
+
+/* ---- electrode surfaces -------------------------------------------------
+ * Replaces the external PyElectrodeAssembly the reference calls each step
+ * (segment_intersects_surface, pusher.py:984): a triangle mesh, copied to the
+ * device with a cell grid over it.  vertices: HOST (n_vertices, 3) float64;
+ * triangles: HOST (n_triangles, 3) int64 vertex indices. */
+typedef struct ppt_surface ppt_surface;   /* opaque */
+
+int ppt_surface_create(int64_t n_vertices, const double* vertices, int64_t n_triangles,
+                       const int64_t* triangles, ppt_surface** out);
+int ppt_surface_destroy(ppt_surface* surface);
+
+/* device bytes held, and the cell grid's dimensions */
+int ppt_surface_info(const ppt_surface* surface, int64_t* bytes, int32_t dims[3]);
+
+/* hit[i] = 1 when the segment p0[i] -> p1[i] meets a triangle (Moller-Trumbore
+ * test, segment parameter 0 <= t <= 1, triangle edges included), else 0.
+ * p0, p1: device (n,3) float64; hit: device uint8[n]. */
+int ppt_surface_segments_hit(const ppt_surface* surface, int64_t n, const double* p0, const double* p1,
+                             uint8_t* hit, void* stream);
 
 /* ---- serving: many jobs per launch -------------------------------------
  * No reference counterpart (the reference runs one track_batch at a time,

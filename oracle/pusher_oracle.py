@@ -81,13 +81,43 @@ def interp3d(pts, grid, values, fill_value=0.0):
     return out
 
 
+def interp1d(x, grid, values, fill_value=0.0):
+    """One component at (M,) coordinates.  interpolators.py:192-205, :239-245."""
+    (gx,) = grid
+    out = np.full(x.shape[0], fill_value, dtype=np.float64)
+    inside = ~((x < gx[0]) | (x > gx[-1]))
+    x = x[inside]
+    i = cell_index(gx, x)
+    t = np.clip((x - gx[i]) / (gx[i + 1] - gx[i]), 0.0, 1.0)
+    out[inside] = values[i] * (1.0 - t) + values[i + 1] * t
+    return out
+
+
+def interp2d(x, y, grid, values, fill_value=0.0):
+    """One component at (M,) x and y.  interpolators.py:208-236, :248-256."""
+    gx, gy = grid
+    out = np.full(x.shape[0], fill_value, dtype=np.float64)
+    inside = ~((x < gx[0]) | (x > gx[-1]) | (y < gy[0]) | (y > gy[-1]))
+    x, y = x[inside], y[inside]
+    i = cell_index(gx, x)
+    j = cell_index(gy, y)
+    tx = np.clip((x - gx[i]) / (gx[i + 1] - gx[i]), 0.0, 1.0)
+    ty = np.clip((y - gy[j]) / (gy[j + 1] - gy[j]), 0.0, 1.0)
+    c0 = values[i, j] * (1.0 - tx) + values[i + 1, j] * tx
+    c1 = values[i, j + 1] * (1.0 - tx) + values[i + 1, j + 1] * tx
+    out[inside] = c0 * (1.0 - ty) + c1 * ty
+    return out
+
+
 # ---------------------------------------------------------------------------
 # Field objects  (field.py:213-244, :441-504, :595-690, :389-407)
 # ---------------------------------------------------------------------------
 
 class MapField:
-    """3D map: per-component trilinear interpolation times ``scaling``
-    (field.py:491-504).  Components given as None are identically zero."""
+    """1D, 2D or 3D map: per-component interpolation times ``scaling``
+    (field.py:457-504).  Components given as None are identically zero.  As
+    in the reference, a 1D map (one grid array) is evaluated at the points'
+    z and a 2D map at their (x, y), whichever axes the grid was given on."""
 
     def __init__(self, grid, values, scaling=1.0):
         self.grid = tuple(np.ascontiguousarray(g, dtype=np.float64) for g in grid)
@@ -103,6 +133,10 @@ class MapField:
         for c in "xyz":
             if self.values[c] is None:
                 cols.append(self.scaling * np.zeros(pts.shape[0]))
+            elif len(self.grid) == 1:
+                cols.append(self.scaling * interp1d(pts[:, 2], self.grid, self.values[c]))
+            elif len(self.grid) == 2:
+                cols.append(self.scaling * interp2d(pts[:, 0], pts[:, 1], self.grid, self.values[c]))
             else:
                 cols.append(self.scaling * interp3d(pts, self.grid, self.values[c]))
         return np.column_stack(cols)
@@ -304,6 +338,12 @@ class _Fields:
         self.efield, self.bfield = efield, bfield
         self.rf = rf  # (omega, phase (M,)) or None
 
+    def subset(self, rows):
+        """The same fields for the particles ``rows`` (their RF phases)."""
+        if self.rf is None:
+            return self
+        return _Fields(self.efield, self.bfield, (self.rf[0], self.rf[1][rows]))
+
     def __call__(self, r, t):
         e = self.efield(r)
         if self.rf is not None:
@@ -378,15 +418,65 @@ def _half_kick(alg, w, e, b, dt, qm):
     return vay_push_u(w, e, b, dt, qm)
 
 
+# ---------------------------------------------------------------------------
+# Electrode surfaces  (pusher.py:966-990; the segment test the external
+# py_electrodes package provides, restated as Moller-Trumbore)
+# ---------------------------------------------------------------------------
+
+def segments_hit(p0, p1, vertices, triangles, chunk=4096):
+    """hit[i]: does the segment p0[i] -> p1[i] meet a triangle?  Moller-Trumbore
+    (J. Graphics Tools 2(1), 1997) with the segment parameter 0 <= t <= 1 and
+    triangle edges included; every product and sum rounded separately, in the
+    order of the device code, so the decisions are the same bit for bit."""
+    p0 = np.asarray(p0, dtype=np.float64).reshape(-1, 3)
+    p1 = np.asarray(p1, dtype=np.float64).reshape(-1, 3)
+    v = np.asarray(vertices, dtype=np.float64)
+    t = np.asarray(triangles, dtype=np.int64)
+    v0 = v[t[:, 0]]
+    e1 = v[t[:, 1]] - v0
+    e2 = v[t[:, 2]] - v0
+    hit = np.zeros(p0.shape[0], dtype=bool)
+
+    def cross(a, b):
+        return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                         a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                         a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1)
+
+    def dot(a, b):
+        return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
+
+    for s in range(0, p0.shape[0], chunk):
+        a = p0[s:s + chunk, None, :]
+        d = (p1[s:s + chunk] - p0[s:s + chunk])[:, None, :]
+        pv = cross(d, e2[None])
+        det = dot(e1[None], pv)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv = 1.0 / det
+            tv = a - v0[None]
+            u = dot(tv, pv) * inv
+            qv = cross(tv, e1[None])
+            w = dot(d, qv) * inv
+            tt = dot(e2[None], qv) * inv
+            ok = (det != 0.0) & (u >= 0.0) & (u <= 1.0) & (w >= 0.0) & (u + w <= 1.0) & (tt >= 0.0) & (tt <= 1.0)
+        hit[s:s + chunk] = ok.any(axis=1)
+    return hit
+
+
 def track_batch(alg, qm, r0, v0, efield, bfield, nsteps, dt, rec_every_n_steps=1,
-                rf=None, t0=0.0):
-    """pusher.py:894-1012 without an electrode assembly (active stays all
-    True).  Returns (r_hist, v_hist, active) with the reference's shapes.
+                rf=None, t0=0.0, surface=None):
+    """pusher.py:894-1012.  Returns (r_hist, v_hist, active) with the
+    reference's shapes.
 
     ``rf=(omega, phase)`` multiplies E by cos(omega t + phase_i).  Field time
     of step n is t0 + n dt; the Boris-family initial half step uses t0 and the
-    final one t0 + nsteps dt.
+    final one t0 + nsteps dt.  ``surface=(vertices, triangles)``: after each
+    step (and its record) the active particles whose step segment meets the
+    surface are deactivated; they are pushed and recorded no more, and the
+    closing half step skips them (pusher.py:966-1007).
     """
+    if surface is not None:
+        return _track_batch_surface(alg, qm, r0, v0, efield, bfield, nsteps, dt, rec_every_n_steps, rf, t0,
+                                    surface)
     m = r0.shape[0]
     n_rec = nsteps // rec_every_n_steps + 1
     r_hist = np.full((n_rec, m, 3), np.nan)
@@ -414,6 +504,44 @@ def track_batch(alg, qm, r0, v0, efield, bfield, nsteps, dt, rec_every_n_steps=1
         e, b = fields(r, t0 + nsteps * dt)
         w = _half_kick(alg, w, e, b, 0.5 * dt, qm)
         v_hist[-1] = as_v(w)
+    return r_hist, v_hist, active
+
+
+def _track_batch_surface(alg, qm, r0, v0, efield, bfield, nsteps, dt, rec_every_n_steps, rf, t0, surface):
+    vertices, triangles = surface
+    m = r0.shape[0]
+    n_rec = nsteps // rec_every_n_steps + 1
+    r_hist = np.full((n_rec, m, 3), np.nan)
+    v_hist = np.full((n_rec, m, 3), np.nan)
+    active = np.ones(m, dtype=bool)
+    fields = _Fields(efield, bfield, rf)
+    r = np.array(r0, dtype=np.float64, copy=True)
+    w = np.array(v0, dtype=np.float64, copy=True)
+    if alg in U_STATE:
+        w = u_from_v(w)
+    as_v = v_from_u if alg in U_STATE else (lambda x: x)
+    if alg in STAGGERED:
+        e, b = fields(r, t0)
+        w = _half_kick(alg, w, e, b, -0.5 * dt, qm)
+    r_hist[0] = r
+    v_hist[0] = as_v(w)
+    rec = 1
+    for step in range(nsteps):
+        rows = np.nonzero(active)[0]
+        if rows.size == 0:
+            break
+        r_old = r[rows].copy()
+        r[rows], w[rows] = push_step(alg, r[rows], w[rows], fields.subset(rows), t0 + step * dt, dt, qm)
+        if (step + 1) % rec_every_n_steps == 0 and rec < n_rec:
+            r_hist[rec][rows] = r[rows]
+            v_hist[rec][rows] = as_v(w[rows])
+            rec += 1
+        active[rows[segments_hit(r_old, r[rows], vertices, triangles)]] = False
+    rows = np.nonzero(active)[0]
+    if alg in STAGGERED and rows.size:
+        e, b = fields.subset(rows)(r[rows], t0 + nsteps * dt)
+        w[rows] = _half_kick(alg, w[rows], e, b, 0.5 * dt, qm)
+        v_hist[-1][rows] = as_v(w[rows])
     return r_hist, v_hist, active
 
 

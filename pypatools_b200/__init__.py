@@ -14,7 +14,8 @@ from .pusher import Pusher, PusherGPU, RFModulation, DeviceTracker
 from .particles import ParticleDistribution
 from .moments import bunch_moments
 from .deposit import bin_particles_cic
+from .electrodes import ElectrodeSurface
 
 __all__ = ["IonSpecies", "PRESETS", "Field", "ScaledField", "CompositeField", "FieldMap", "get_interpolator",
            "CudaInterpolator", "Pusher", "PusherGPU", "RFModulation", "DeviceTracker", "ParticleDistribution",
-           "bunch_moments", "bin_particles_cic"]
+           "bunch_moments", "bin_particles_cic", "ElectrodeSurface"]

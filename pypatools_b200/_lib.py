@@ -56,7 +56,7 @@ class TrackArgs(ctypes.Structure):
                 ("dt", c_double), ("q_over_m", c_double), ("t0", c_double),
                 ("rf_omega", c_double), ("rf_phase", c_void_p), ("r_hist", c_void_p),
                 ("v_hist", c_void_p), ("order", c_void_p), ("status", c_void_p),
-                ("counters", c_void_p)]
+                ("counters", c_void_p), ("surface", c_void_p), ("active", c_void_p)]
 
 
 class JobDesc(ctypes.Structure):
@@ -75,6 +75,10 @@ SIGNATURES = {
     "ppt_fieldmap_create": (c_int, [POINTER(GridDesc), c_int, c_int, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_layout": (c_int, [c_uint32]),
     "ppt_deposit_cic": (c_int, [c_int64, c_void_p, c_void_p, POINTER(MeshDesc), c_void_p, c_void_p]),
+    "ppt_surface_create": (c_int, [c_int64, c_void_p, c_int64, c_void_p, POINTER(c_void_p)]),
+    "ppt_surface_destroy": (c_int, [c_void_p]),
+    "ppt_surface_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32)]),
+    "ppt_surface_segments_hit": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_fieldmap_create_masked": (c_int, [POINTER(GridDesc), c_uint32, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_add": (c_int, [c_void_p, POINTER(c_void_p * 6), POINTER(c_double * 6), c_int, c_void_p]),
     "ppt_fieldmap_destroy": (c_int, [c_void_p]),
@@ -113,7 +117,7 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.ppt_abi_version() != 1:
+    if lib.ppt_abi_version() != 2:
         raise ImportError("libppt.so ABI version mismatch; rebuild it")
     _lib = lib
     return lib

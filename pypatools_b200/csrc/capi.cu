@@ -80,8 +80,15 @@ extern "C" int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_trac
         P.order = a->order;
         P.status = a->status;
         P.counters = a->counters;
-        return launch_track_f64(P, st->algorithm, rf, s);
+        if (a->surface) {
+            if (!a->active) return fail(PPT_ERR_ARG, "a surface needs the active array");
+            P.surf = a->surface->dev;
+            P.active = a->active;
+        }
+        return launch_track_f64(P, st->algorithm, rf, a->surface != nullptr, s);
     }
+    if (a->surface)
+        return fail(PPT_ERR_UNSUPPORTED, "electrode surfaces run in the float64 form only");
     TrackMixDev P;
     std::memset(&P, 0, sizeof(P));
     rc = make_track_mixed(F, st, a, n_rec, &P);

@@ -61,6 +61,28 @@ __global__ void map_add_kernel(Dst* __restrict__ dst, int stride, int slot,
     }
 }
 
+// The same for a map with axes it does not vary along: stored node (I, J, K)
+// reads the caller's node (i, j, k), i = 0 on such an axis (both stored
+// layers get the one source value).
+struct FlatIndex {
+    int64_t n1, n2;         // stored node layers of y and z
+    int64_t src1, src2;     // caller's node counts of y and z
+    int flat[3];
+};
+
+template <typename Dst, typename Src>
+__global__ void map_add_flat_kernel(Dst* __restrict__ dst, int stride, int slot, const Src* __restrict__ src,
+                                    double scale, int64_t nodes, FlatIndex X) {
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t step = (int64_t)gridDim.x * blockDim.x;
+    for (; p < nodes; p += step) {
+        const int64_t K = p % X.n2, J = (p / X.n2) % X.n1, I = p / (X.n1 * X.n2);
+        const int64_t i = X.flat[0] ? 0 : I, j = X.flat[1] ? 0 : J, k = X.flat[2] ? 0 : K;
+        Dst* q = dst + p * stride + slot;
+        *q = (Dst)((double)*q + scale * (double)src[(i * X.src1 + j) * X.src2 + k]);
+    }
+}
+
 int build_fields(const ppt_fields* f, FieldsDev* out) {
     if (!f) return fail(PPT_ERR_ARG, "fields is NULL");
     if (f->n_maps < 0 || f->n_maps > PPT_MAX_MAPS)
@@ -152,6 +174,29 @@ __device__ __forceinline__ float tri_f(float c000, float c100, float c010, float
     return fmaf(c1 - c0, tz, c0);
 }
 
+template <typename Dst, typename Src>
+void launch_map_add(const ppt_fieldmap* map, Dst* dst, int slot, const Src* src, double scale, cudaStream_t s) {
+    const int64_t nodes = map->n[0] * map->n[1] * map->n[2];
+    const int block = 256;
+    const int64_t g = (nodes + block - 1) / block;
+    const int grid = (int)(g > 148 * 32 ? 148 * 32 : g);
+    FlatIndex X;
+    bool any_flat = false;
+    for (int d = 0; d < 3; ++d) {
+        X.flat[d] = map->src_n[d] == 1 && map->n[d] == 2;
+        any_flat |= X.flat[d] != 0;
+    }
+    if (!any_flat) {
+        map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot, src, scale, nodes);
+        return;
+    }
+    X.n1 = map->n[1];
+    X.n2 = map->n[2];
+    X.src1 = map->src_n[1];
+    X.src2 = map->src_n[2];
+    map_add_flat_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot, src, scale, nodes, X);
+}
+
 }  // namespace ppt
 
 using namespace ppt;
@@ -182,11 +227,29 @@ extern "C" int ppt_fieldmap_create_masked(const ppt_grid_desc* grid, uint32_t co
     ppt_fieldmap m;
     std::memset(&m, 0, sizeof(m));
     int64_t total_nodes = 1;
+    int flat_axes = 0;
     std::vector<double> axes;
     for (int d = 0; d < 3; ++d) {
         int64_t n = grid->n[d];
-        if (n < 2) return fail(PPT_ERR_ARG, "every axis needs at least 2 nodes");
+        if (n < 1) return fail(PPT_ERR_ARG, "every axis needs at least 1 node");
         if (n > (1LL << 30)) return fail(PPT_ERR_ARG, "axis too long");
+        m.src_n[d] = n;
+        if (n == 1) {
+            // the map does not vary along this axis (a 1D or 2D field)
+            AxisDev& a = m.dev.ax[d];
+            a.n = 2;
+            a.lo = -kFlatHalf;
+            a.hi = kFlatHalf;
+            a.d = 2.0 * kFlatHalf;
+            a.inv_d = 0.5 / kFlatHalf;
+            a.uniform = 1;
+            m.n[d] = 2;
+            total_nodes *= 2;
+            axes.push_back(a.lo);
+            axes.push_back(a.hi);
+            ++flat_axes;
+            continue;
+        }
         if (!grid->axis[d]) return fail(PPT_ERR_ARG, "grid axis pointer is NULL");
         const double* g = grid->axis[d];
         for (int64_t i = 1; i < n; ++i)
@@ -209,6 +272,7 @@ extern "C" int ppt_fieldmap_create_masked(const ppt_grid_desc* grid, uint32_t co
         total_nodes *= n;
         axes.insert(axes.end(), g, g + n);
     }
+    if (flat_axes == 3) return fail(PPT_ERR_ARG, "a map needs an axis with at least 2 nodes (use constants)");
     m.dev.all_uniform = m.dev.ax[0].uniform && m.dev.ax[1].uniform && m.dev.ax[2].uniform;
     if (store_dtype == PPT_DTYPE_F32 && !m.dev.all_uniform)
         return fail(PPT_ERR_UNSUPPORTED, "float32 (mixed-precision) maps need uniform grid axes");
@@ -256,10 +320,6 @@ extern "C" int ppt_fieldmap_add(ppt_fieldmap* map, const void* const comp[6], co
     if (src_dtype != PPT_DTYPE_F64 && src_dtype != PPT_DTYPE_F32)
         return fail(PPT_ERR_ARG, "src_dtype must be PPT_DTYPE_F64 or PPT_DTYPE_F32");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int64_t nodes = map->n[0] * map->n[1] * map->n[2];
-    const int block = 256;
-    int64_t g = (nodes + block - 1) / block;
-    const int grid = (int)(g > 148 * 32 ? 148 * 32 : g);
     for (int c = 0; c < 6; ++c) {
         if (!comp[c]) continue;
         const int slot = layout_slot(map->dev.layout, c);
@@ -267,23 +327,15 @@ extern "C" int ppt_fieldmap_add(ppt_fieldmap* map, const void* const comp[6], co
             static const char* names[6] = {"Ex", "Ey", "Ez", "Bx", "By", "Bz"};
             return fail(PPT_ERR_ARG, std::string("the map's layout does not store ") + names[c]);
         }
-        if (map->dev.dtype == PPT_DTYPE_F64) {
-            double* dst = static_cast<double*>(map->data);
-            if (src_dtype == PPT_DTYPE_F64)
-                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
-                                                      static_cast<const double*>(comp[c]), scale[c], nodes);
-            else
-                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
-                                                      static_cast<const float*>(comp[c]), scale[c], nodes);
-        } else {
-            float* dst = static_cast<float*>(map->data);
-            if (src_dtype == PPT_DTYPE_F64)
-                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
-                                                      static_cast<const double*>(comp[c]), scale[c], nodes);
-            else
-                map_add_kernel<<<grid, block, 0, s>>>(dst, map->dev.stride, slot,
-                                                      static_cast<const float*>(comp[c]), scale[c], nodes);
-        }
+        const bool f64_dst = map->dev.dtype == PPT_DTYPE_F64, f64_src = src_dtype == PPT_DTYPE_F64;
+        double* d64 = static_cast<double*>(map->data);
+        float* d32 = static_cast<float*>(map->data);
+        const double* s64 = static_cast<const double*>(comp[c]);
+        const float* s32 = static_cast<const float*>(comp[c]);
+        if (f64_dst && f64_src) launch_map_add(map, d64, slot, s64, scale[c], s);
+        else if (f64_dst) launch_map_add(map, d64, slot, s32, scale[c], s);
+        else if (f64_src) launch_map_add(map, d32, slot, s64, scale[c], s);
+        else launch_map_add(map, d32, slot, s32, scale[c], s);
         PPT_CUDA_TRY(cudaGetLastError());
     }
     return PPT_OK;

@@ -48,6 +48,18 @@ struct AxisDev {
     int uniform;
 };
 
+// An axis along which a map does not vary (the reference's 1D fields vary
+// along z only, its 2D fields along x and y: field.py:457-489) is stored as
+// two identical node layers at -2^996 and +2^996: every finite coordinate is
+// inside, the uniform cell search gives cell 0 and weight exactly 1/2, and
+// the lerp of two equal values is exact, so the 3D interpolation reduces
+// bit for bit to the 1D / 2D one without a branch in the kernels.
+constexpr double kFlatHalf = 0x1p996;
+
+__host__ __device__ __forceinline__ bool axis_is_flat(const AxisDev& a) {
+    return a.n == 2 && a.lo == -kFlatHalf && a.hi == kFlatHalf;
+}
+
 // Record layouts, named by the component mask they store (bit c = Ex, Ey,
 // Ez, Bx, By, Bz).  Up to three components are packed in Ex..Bz order in
 // records of 1, 2 or 4 elements; all six use [Ex Ey Ez 0 | Bx By Bz 0].
@@ -87,7 +99,8 @@ struct ppt_fieldmap {
     double* axis_buf;     // device node coordinates of all three axes
     void* data;
     size_t bytes;
-    int64_t n[3];
+    int64_t n[3];     // stored node layers per axis (2 for an axis the map does not vary along)
+    int64_t src_n[3]; // node counts of the caller's arrays (1 for such an axis)
 };
 
 namespace ppt {

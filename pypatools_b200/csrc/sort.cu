@@ -31,6 +31,7 @@ struct SortGeom {
     int n[3];           // nodes per axis
     uint32_t n_in;      // buckets for in-map cells
     uint32_t outside;   // bucket of particles outside the map (= n_in)
+    int flat[3];        // the map does not vary along the axis: its cell is not part of the key
 };
 
 __device__ __forceinline__ bool cell_inside(const SortGeom& G, int c0, int c1, int c2) {
@@ -92,7 +93,9 @@ __global__ void sort_keys_mixed(int64_t n, const int32_t* __restrict__ ci, SortG
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     uint32_t b = G.outside;
     if (s < n) {
-        b = bucket_of_cells(G, ci[s], ci[n + s], ci[2 * n + s]);
+        // mixed-form cells on an axis the map does not vary along count
+        // on their own grid, not the map's single layer
+        b = bucket_of_cells(G, G.flat[0] ? 0 : ci[s], G.flat[1] ? 0 : ci[n + s], G.flat[2] ? 0 : ci[2 * n + s]);
         key[s] = b;
     }
     count_key(b, s < n && b != G.outside, count, ctrl);
@@ -260,6 +263,7 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
         G.lo[a] = m.ax[a].lo;
         G.inv_d[a] = m.ax[a].inv_d;
         G.n[a] = m.ax[a].n;
+        G.flat[a] = axis_is_flat(m.ax[a]) ? 1 : 0;
         cells *= (uint64_t)(m.ax[a].n - 1);
     }
     G.n_in = (uint32_t)(cells < ((uint64_t)1 << kBucketBits) ? cells : ((uint64_t)1 << kBucketBits));

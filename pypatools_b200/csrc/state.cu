@@ -1,6 +1,7 @@
 // Conversion between the reference's (M,3) float64 r / v arrays
 // (Pusher.track_batch inputs and outputs, src/PyPATools/pusher.py:894-1012)
 // and the device structure-of-arrays particle state the track kernels keep.
+#include <algorithm>
 #include <cmath>
 
 #include "ppt_internal.cuh"
@@ -108,7 +109,22 @@ int mixed_grid(const FieldsDev& F, GridF* G) {
     const MapDev& m = F.maps[0];
     if (m.dtype != PPT_DTYPE_F32) return fail(PPT_ERR_ARG, "the mixed form needs a float32 map");
     if (!m.all_uniform) return fail(PPT_ERR_UNSUPPORTED, "the mixed form needs uniform grid axes");
+    // Along an axis the map does not vary, positions still need cells: a
+    // grid of 2^24 cells of the finest spacing of the other axes, centred on
+    // 0 (every cell of it reads the map's one layer; make_track_mixed zeroes
+    // the map stride of that axis).  Cell indices stay below 2^24, exact in
+    // float32 as the kernels need.
+    double fine = 0.0;
+    for (int c = 0; c < 3; ++c)
+        if (!axis_is_flat(m.ax[c])) fine = fine == 0.0 ? m.ax[c].d : std::min(fine, m.ax[c].d);
     for (int c = 0; c < 3; ++c) {
+        if (axis_is_flat(m.ax[c])) {
+            G->d[c] = fine;
+            G->inv_d[c] = 1.0 / fine;
+            G->lo[c] = -(double)(1 << 23) * fine;
+            G->n[c] = (1 << 24) + 1;
+            continue;
+        }
         G->lo[c] = m.ax[c].lo;
         G->d[c] = m.ax[c].d;
         G->inv_d[c] = m.ax[c].inv_d;

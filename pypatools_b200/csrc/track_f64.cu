@@ -275,15 +275,21 @@ __device__ __forceinline__ Ctx make_ctx(const TrackDev& P) {
 }
 
 // All steps of one call for particle slot s (s < P.n); returns the steps done.
-template <int ALG, bool RF>
+// COLL: each step's segment is tested against the electrode surface after the
+// step's snapshot, and a particle that hits stops there (pusher.py:966-990).
+template <int ALG, bool RF, bool COLL>
 __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_t s, Ctx& c) {
     {
         const int64_t n = P.n;
         double* st = P.f64;
+        const int64_t row = P.order ? P.order[s] : s;
+        if constexpr (COLL) {
+            if (!P.active[row]) return 0;   // stopped in an earlier call: nothing moves or records
+        }
         V3 r = v3(st[s], st[n + s], st[2 * n + s]);
         V3 w = v3(st[3 * n + s], st[4 * n + s], st[5 * n + s]);
-        const int64_t row = P.order ? P.order[s] : s;
         if (RF) c.phase = P.rf_phase[s];
+        bool stopped = false;
 
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (alg_staggered(ALG)) {
@@ -308,6 +314,33 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
             const int64_t to_rec = (int64_t)until + 1;
             const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
             const int64_t g0 = P.step0 + k;
+            if constexpr (COLL) {
+                // one step at a time, each segment tested (no field-free runs)
+                int i = 0;
+                while (i < seg) {
+                    const V3 r0 = r;
+                    step<ALG, RF>(c, r, w, g0 + i);
+                    ++i;
+                    if (segment_hits_surface(P.surf, r0, r)) {
+                        stopped = true;
+                        break;
+                    }
+                }
+                k += i;
+                // the reference records the step's position before its collision test
+                if ((int64_t)i == to_rec) {
+                    const int64_t rec = (P.step0 + k) / P.rec_every;
+                    if (P.r_hist && rec < P.n_rec) {
+                        write_row(P.r_hist, rec, n, row, r);
+                        write_row(P.v_hist, rec, n, row, w_to_v<ALG>(w));
+                    }
+                    until = rec_every - 1;
+                } else {
+                    until -= i;
+                }
+                if (stopped) break;
+                continue;
+            }
             if constexpr (alg_skips_free(ALG)) {
                 for (int i = 0; i < seg;) {
                     if (quiet > 0) {
@@ -338,7 +371,7 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
                 until -= seg;
             }
         }
-        if (P.flags & PPT_TRACK_FINAL) {
+        if ((P.flags & PPT_TRACK_FINAL) && !stopped) {
             if constexpr (alg_staggered(ALG)) {
                 V3 E, B;
                 fields_at<RF>(c, r, P.nsteps_total, 0.0, E, B);
@@ -356,16 +389,22 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
             double sum = r.x + r.y + r.z + w.x + w.y + w.z;
             if (!isfinite(sum)) atomicOr(P.status, PPT_STATUS_NONFINITE);
         }
+        if constexpr (COLL) {
+            if (stopped) {
+                P.active[row] = 0;
+                return (unsigned)k;
+            }
+        }
     }
     return (unsigned)P.nsteps;
 }
 
-template <int ALG, bool RF>
+template <int ALG, bool RF, bool COLL>
 __global__ void __launch_bounds__(128, alg_skips_free(ALG) ? 5 : 1) track_f64_kernel(const __grid_constant__ TrackDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
     Ctx c = make_ctx(P);
-    if (s < P.n) steps_done = track_f64_particle<ALG, RF>(P, s, c);
+    if (s < P.n) steps_done = track_f64_particle<ALG, RF, COLL>(P, s, c);
     if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
 }
 
@@ -405,7 +444,7 @@ __global__ void __launch_bounds__(kJobBlock) track_f64_jobs_kernel(const __grid_
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
             Ctx c = make_ctx(sP);
             unsigned sd = 0;
-            if (s < sP.n) sd = track_f64_particle<ALG, RF>(sP, s, c);
+            if (s < sP.n) sd = track_f64_particle<ALG, RF, false>(sP, s, c);
             if (sP.counters) block_add_counters(sP.counters, c.hits, sd);
         }
         __syncthreads();
@@ -438,26 +477,31 @@ int launch_f64_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cuda
 }
 
 template <int ALG>
-static cudaError_t launch_alg(const TrackDev& P, bool rf, cudaStream_t s) {
+static cudaError_t launch_alg(const TrackDev& P, bool rf, bool coll, cudaStream_t s) {
     const int block = pick_block(P.n);
     const int grid = grid_for(P.n, block);
-    if (rf) track_f64_kernel<ALG, true><<<grid, block, 0, s>>>(P);
-    else track_f64_kernel<ALG, false><<<grid, block, 0, s>>>(P);
+    if (coll) {
+        if (rf) track_f64_kernel<ALG, true, true><<<grid, block, 0, s>>>(P);
+        else track_f64_kernel<ALG, false, true><<<grid, block, 0, s>>>(P);
+    } else {
+        if (rf) track_f64_kernel<ALG, true, false><<<grid, block, 0, s>>>(P);
+        else track_f64_kernel<ALG, false, false><<<grid, block, 0, s>>>(P);
+    }
     return cudaGetLastError();
 }
 
-int launch_track_f64(const TrackDev& P, int algorithm, bool rf, cudaStream_t s) {
+int launch_track_f64(const TrackDev& P, int algorithm, bool rf, bool coll, cudaStream_t s) {
     cudaError_t e;
     switch (algorithm) {
-        case PPT_ALG_LEAPFROG: e = launch_alg<PPT_ALG_LEAPFROG>(P, rf, s); break;
-        case PPT_ALG_BORIS: e = launch_alg<PPT_ALG_BORIS>(P, rf, s); break;
-        case PPT_ALG_RK4: e = launch_alg<PPT_ALG_RK4>(P, rf, s); break;
-        case PPT_ALG_YOSHIDA: e = launch_alg<PPT_ALG_YOSHIDA>(P, rf, s); break;
-        case PPT_ALG_VAY_REL: e = launch_alg<PPT_ALG_VAY_REL>(P, rf, s); break;
-        case PPT_ALG_RK4_REL: e = launch_alg<PPT_ALG_RK4_REL>(P, rf, s); break;
-        case PPT_ALG_YOSHIDA_REL: e = launch_alg<PPT_ALG_YOSHIDA_REL>(P, rf, s); break;
-        case PPT_ALG_BORIS_REL: e = launch_alg<PPT_ALG_BORIS_REL>(P, rf, s); break;
-        case PPT_ALG_VAY: e = launch_alg<PPT_ALG_VAY>(P, rf, s); break;
+        case PPT_ALG_LEAPFROG: e = launch_alg<PPT_ALG_LEAPFROG>(P, rf, coll, s); break;
+        case PPT_ALG_BORIS: e = launch_alg<PPT_ALG_BORIS>(P, rf, coll, s); break;
+        case PPT_ALG_RK4: e = launch_alg<PPT_ALG_RK4>(P, rf, coll, s); break;
+        case PPT_ALG_YOSHIDA: e = launch_alg<PPT_ALG_YOSHIDA>(P, rf, coll, s); break;
+        case PPT_ALG_VAY_REL: e = launch_alg<PPT_ALG_VAY_REL>(P, rf, coll, s); break;
+        case PPT_ALG_RK4_REL: e = launch_alg<PPT_ALG_RK4_REL>(P, rf, coll, s); break;
+        case PPT_ALG_YOSHIDA_REL: e = launch_alg<PPT_ALG_YOSHIDA_REL>(P, rf, coll, s); break;
+        case PPT_ALG_BORIS_REL: e = launch_alg<PPT_ALG_BORIS_REL>(P, rf, coll, s); break;
+        case PPT_ALG_VAY: e = launch_alg<PPT_ALG_VAY>(P, rf, coll, s); break;
         default: return fail(PPT_ERR_ARG, "unknown algorithm");
     }
     if (e != cudaSuccess) return cuda_fail(e, "track_f64_kernel launch");

@@ -115,7 +115,9 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     const float w[8] = {a00 * uz, a00 * tz, a01 * uz, a01 * tz, a10 * uz, a10 * tz, a11 * uz, a11 * tz};
     constexpr int W = layout_width(L);
     // corner (di, dj) = (0,0) (0,1) (1,0) (1,1); the k+1 corner is the next
-    // record; 32-bit offsets when the map's elements allow (maps below 2^31)
+    // record; 32-bit offsets when the map's elements allow (maps below 2^31
+    // that vary along z: a map constant along z takes the 64-bit path, whose
+    // z stride k_elems is 0 for it, so the common path keeps k * W)
     const float* p00;
     const float* p10;
     const float* p01;
@@ -125,8 +127,8 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
         p10 = p00 + sx;
         p01 = p00 + sy;
     } else {
-        const int64_t node = (int64_t)i * m.sx + (int64_t)j * m.sy + k;
-        p00 = static_cast<const float*>(m.data) + node * W;
+        const int64_t off = ((int64_t)i * m.sx + (int64_t)j * m.sy) * W + (int64_t)k * P.k_elems;
+        p00 = static_cast<const float*>(m.data) + off;
         p10 = p00 + m.sx * W;
         p01 = p00 + m.sy * W;
     }
@@ -825,6 +827,11 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
     int rc = mixed_grid(F, &P->G);
     if (rc) return rc;
     P->map = F.maps[0];
+    // an axis the map does not vary along: every cell reads its one layer
+    if (axis_is_flat(P->map.ax[0])) P->map.sx = 0;
+    if (axis_is_flat(P->map.ax[1])) P->map.sy = 0;
+    P->k_elems = axis_is_flat(P->map.ax[2]) ? 0 : layout_width(P->map.layout);
+    if (P->k_elems == 0) P->map.idx32 = 0;
     for (int c = 0; c < 3; ++c) {
         P->e_const[c] = (float)F.e_const[c];
         P->b_const[c] = (float)F.b_const[c];

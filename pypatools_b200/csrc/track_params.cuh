@@ -3,6 +3,7 @@
 #pragma once
 
 #include "mixed_common.cuh"
+#include "surface.cuh"
 
 namespace ppt {
 
@@ -26,6 +27,8 @@ struct TrackDev {
     const int64_t* order;
     int* status;
     unsigned long long* counters;
+    SurfaceDev surf;    // electrode surface (n_tri = 0: none)
+    uint8_t* active;    // row order; with a surface, 0 = stopped by it
 };
 
 struct TrackMixDev {
@@ -62,6 +65,7 @@ struct TrackMixDev {
     unsigned long long* counters;
     int32_t rf_tab_n;   // entries of the per-step RF table a launch builds (0: none)
     float wscale;       // Boris: (0.5 q/m dt) / hqdt - 1, applied to each velocity increment
+    int32_t k_elems;    // map elements per z cell: the record width, 0 when the map does not vary along z
 };
 
 // One (form, algorithm, RF) class of serving jobs: a block-level work queue
@@ -85,7 +89,7 @@ constexpr int kJobBlock = 128;
 
 int mixed_grid(const FieldsDev& F, GridF* G);
 int check_state(const ppt_state* st);
-int launch_track_f64(const TrackDev& P, int algorithm, bool rf, cudaStream_t s);
+int launch_track_f64(const TrackDev& P, int algorithm, bool rf, bool surface, cudaStream_t s);
 int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_args* a, int64_t n_rec,
                      TrackMixDev* P);
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s);

@@ -11,6 +11,11 @@ package's classes and the reference's own, by duck typing):
   ``_values``), scipy ``RegularGridInterpolator`` (``grid``, ``values``),
   this package's ``CudaInterpolator``; the field's ``_scaling`` multiplies
   them (field.py:491-504);
+* ``Field`` of dim 1 or 2 with such interpolators: a dim-1 field varies
+  along z only and a dim-2 field along x and y, whatever axes its grid was
+  given on (``_get_field_1d`` / ``_get_field_2d`` evaluate the interpolators
+  at ``pts[:, 2]`` and ``pts[:, :2]``, field.py:457-489); it becomes a map
+  with one-node axes, which the kernels treat as unbounded and constant;
 * ``Field.zero()`` (field.py:389-407) -> nothing;
 * ``ScaledField`` (scale * F + offset, field.py:661-690);
 * ``CompositeField`` (sum of w_i F_i, field.py:595-658);
@@ -104,6 +109,20 @@ def _all_zero(values):
     return result
 
 
+_ONE_NODE = np.zeros(1)
+
+
+def _as_3d(grid):
+    """The grid of a 1D (z) or 2D (x, y) interpolator as a 3D node grid whose
+    other axes have one node (field.py:457-489).  The node values keep their
+    shape: flattened in C order they are already the 3D map's [i][j][k]."""
+    if len(grid) == 1:
+        return (_ONE_NODE, _ONE_NODE, grid[0])
+    if len(grid) == 2:
+        return (grid[0], grid[1], _ONE_NODE)
+    return grid
+
+
 def decompose(field):
     """Field-like object -> FieldTerms."""
     out = FieldTerms()
@@ -126,8 +145,8 @@ def decompose(field):
         if dim == 0:
             out.const = scaling * np.array([float(comps[c] or 0.0) for c in "xyz"])
             return out
-        if dim != 3:
-            raise NotImplementedError(f"{dim}D fields are not on the GPU path (3D maps and constants are)")
+        if dim not in (1, 2, 3):
+            raise NotImplementedError(f"{dim}D fields are not on the GPU path")
         grid = None
         values = {}
         for c in "xyz":
@@ -136,8 +155,9 @@ def decompose(field):
                 values[c] = None
                 continue
             g, v = gv
-            if len(g) != 3:
-                raise NotImplementedError("3D fields need 3D component interpolators")
+            if len(g) != dim:
+                raise NotImplementedError(f"a {dim}D field needs {dim}D component interpolators")
+            g = _as_3d(g)
             if grid is None:
                 grid = g
             elif not all(np.array_equal(a, b) for a, b in zip(grid, g)):
@@ -152,7 +172,7 @@ def decompose(field):
         return out
     raise NotImplementedError(
         f"field of type {type(field).__name__} cannot be evaluated on the GPU: pass a Field "
-        "(dim 0 or 3), ScaledField or CompositeField built from node maps")
+        "(dim 0 to 3), ScaledField or CompositeField built from node maps")
 
 
 def _grid_key(grid):

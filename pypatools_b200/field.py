@@ -3,13 +3,14 @@
 Mirrors ``Field``, ``ScaledField``, ``CompositeField``, ``FieldMap`` and
 ``get_interpolator`` of the reference (src/PyPATools/field.py:101-755,
 field_src/interpolators.py:533-610) for the pieces on the pusher path:
-0D (constant) and 3D node-map fields, field algebra, and point evaluation.
-Evaluation goes through ``ppt_field_eval`` (one cell lookup per point for
-all components) instead of three per-component Numba passes.
+0D (constant) fields and 1D, 2D and 3D node-map fields, field algebra, and
+point evaluation.  Evaluation goes through ``ppt_field_eval`` (one cell
+lookup per point for all components) instead of three per-component Numba
+passes.  As in the reference, a 1D field varies along z and a 2D field along
+x and y (field.py:457-489).
 
 The pusher accepts these objects and the reference's own equally (see
-``device_fields``).  File loaders and 1D/2D fields are not part of this
-package.
+``device_fields``).  File loaders are not part of this package.
 """
 import numpy as np
 
@@ -68,7 +69,7 @@ class FieldBase:
 
 
 class Field(FieldBase):
-    """0D constant or 3D node-map field (field.py:101-560 API)."""
+    """0D constant or 1D / 2D / 3D node-map field (field.py:101-560 API)."""
 
     def __init__(self, label="Field", dim=0, field=None, scaling=1.0, units="m", debug=False,
                  method="linear", interpolator_backend="auto"):
@@ -93,7 +94,7 @@ class Field(FieldBase):
         if self._dim == 0:
             m = pts.shape[0]
             return np.column_stack([self._scaling * self._field[c] * np.ones(m) for c in "xyz"])
-        if self._dim != 3:
+        if self._dim not in (1, 2, 3):
             raise NotImplementedError(f"{self._dim}D fields are not supported by this package")
         return _evaluate(self, pts)
 
@@ -206,16 +207,16 @@ class FieldMap:
 
 
 class CudaInterpolator:
-    """Trilinear interpolation of one component on the GPU
-    (the 'cuda' backend of ``get_interpolator``; the API of
-    ``NumbaInterpolator``, field_src/interpolators.py:273-408)."""
+    """Linear / bilinear / trilinear interpolation of one component on the
+    GPU (the 'cuda' backend of ``get_interpolator``; the API of
+    ``NumbaInterpolator``, field_src/interpolators.py:273-408, 1 to 3 axes)."""
 
     def __init__(self, points, values, method="linear", bounds_error=True, fill_value=np.nan):
         if method != "linear":
             raise ValueError(f"Method '{method}' not supported. Use 'linear'")
         self.ndim = len(points)
-        if self.ndim != 3:
-            raise NotImplementedError("the GPU interpolator is 3D")
+        if self.ndim not in (1, 2, 3):
+            raise ValueError(f"Only 1D, 2D, 3D supported. Got {self.ndim}D")
         self.method = method
         self.bounds_error = bounds_error
         self.fill_value = float(fill_value)
@@ -238,8 +239,15 @@ class CudaInterpolator:
             for i, (lo, hi) in enumerate(self._bounds):
                 if np.any(xi[:, i] < lo) or np.any(xi[:, i] > hi):
                     raise ValueError("One or more points are outside the interpolation domain")
-        one = Field(dim=3, field={"x": _Plain(self), "y": None, "z": None})
-        out = _evaluate(one, xi)[:, 0]
+        # a one-component Field of the same dimension: its 1D axis is z, its
+        # 2D axes are x and y (field.py:457-489)
+        pts = np.zeros((xi.shape[0], 3))
+        if self.ndim == 1:
+            pts[:, 2] = xi[:, 0]
+        else:
+            pts[:, :self.ndim] = xi
+        one = Field(dim=self.ndim, field={"x": _Plain(self), "y": None, "z": None})
+        out = _evaluate(one, pts)[:, 0]
         if self.fill_value != 0.0:
             outside = np.zeros(xi.shape[0], dtype=bool)
             for i, (lo, hi) in enumerate(self._bounds):

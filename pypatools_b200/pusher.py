@@ -18,7 +18,9 @@ in float64, the drop-in; 'mixed' = the mixed-precision form), ``device``,
 tensors), ``steps_per_launch``, ``sort_every`` (cell re-sort interval; 'auto' = every 300
 steps for bunches of 65536 or more, none below) and,
 on ``track_batch``, ``rf`` (an ``RFModulation`` multiplying E by
-cos(2 pi f t + phi_i)) and ``t0``.
+cos(2 pi f t + phi_i)) and ``t0``.  ``electrode_assembly`` takes an
+``electrodes.ElectrodeSurface`` (or any object with ``vertices`` and
+``triangles``): particles whose step meets it stop, as in the reference.
 
 All work runs in libppt.so kernels; there is no CPU fallback.
 """
@@ -75,7 +77,7 @@ class DeviceTracker:
 
     def __init__(self, algorithm, q_over_m, dfields, n, nsteps_total, dt, rec_every=1, precision="fp64",
                  rf_omega=0.0, rf_phase=None, t0=0.0, record=True, stagger=True, counters=False,
-                 device=None):
+                 device=None, surface=None):
         torch = _torch()
         self.torch = torch
         if algorithm not in _lib.ALG_IDS:
@@ -114,9 +116,22 @@ class DeviceTracker:
                                 self.f64.data_ptr() if self.f64 is not None else None,
                                 self.i32.data_ptr() if self.i32 is not None else None,
                                 self.f32.data_ptr() if self.f32 is not None else None)
+        # an electrode surface (float64 form): particles whose step segment
+        # meets it stop; active[row] says which are still tracked
+        self.surface = None
+        self.active = None
+        if surface is not None:
+            if precision != "fp64":
+                raise NotImplementedError("electrode surfaces run in the float64 form; use precision='fp64'")
+            self.surface = surface.handle(dev)
+            self.active = torch.ones(n, dtype=torch.uint8, device=dev)
         if record:
-            self.r_hist = torch.empty((self.n_rec, n, 3), dtype=torch.float64, device=dev)
-            self.v_hist = torch.empty((self.n_rec, n, 3), dtype=torch.float64, device=dev)
+            # stopped particles leave their later rows unwritten: NaN, as the
+            # reference's histories start (pusher.py:947-948)
+            make = torch.full if surface is not None else torch.empty
+            args = (float("nan"),) if surface is not None else ()
+            self.r_hist = make((self.n_rec, n, 3), *args, dtype=torch.float64, device=dev)
+            self.v_hist = make((self.n_rec, n, 3), *args, dtype=torch.float64, device=dev)
         else:
             self.r_hist = self.v_hist = None
         self.rf_omega = float(rf_omega)
@@ -168,6 +183,9 @@ class DeviceTracker:
         a.order = self.order.data_ptr() if self.order is not None else None
         a.status = self.status.data_ptr()
         a.counters = self.counters.data_ptr() if self.counters is not None else None
+        if self.surface is not None:
+            a.surface = self.surface
+            a.active = self.active.data_ptr()
         _lib.check(self.lib.ppt_track(self.state, self.dfields.fields, a, self._stream(stream)))
         if k > 0 or flags:
             self.launches += 1
@@ -302,9 +320,12 @@ class PusherGPU:
             warnings.warn("Leapfrog is non-relativistic. Using 'vay_rel' instead for better relativistic "
                           "accuracy.", UserWarning)
             algorithm = "vay_rel"
-        if electrode_assembly:
-            raise NotImplementedError("electrode collision termination is not on the GPU path; "
-                                      "track without an electrode assembly")
+        self.surface = None
+        if electrode_assembly is not None:
+            from .electrodes import ElectrodeSurface
+            self.surface = ElectrodeSurface.from_assembly(electrode_assembly)
+            if precision != "fp64":
+                raise NotImplementedError("electrode surfaces run in the float64 form; use precision='fp64'")
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if snapshot not in ("host", "device"):
@@ -379,10 +400,12 @@ class PusherGPU:
         return d_r.cpu().numpy(), d_v.cpu().numpy()
 
     def track_batch(self, r0_array, v0_array, efield, bfield, nsteps, dt, rec_every_n_steps=1, verbose=False,
-                    *, rf=None, t0=0.0):
+                    *, rf=None, t0=0.0, _collide=True):
         """Track M particles (pusher.py:894-1012).  Returns
         (r_hist (n_rec, M, 3), v_hist, active (M,)) with
-        n_rec = nsteps // rec_every_n_steps + 1."""
+        n_rec = nsteps // rec_every_n_steps + 1.  With an electrode assembly,
+        a particle whose step meets it stops after that step (its later rows
+        stay NaN, no closing half step) and is False in ``active``."""
         if not np.isscalar(dt):
             raise TypeError("dt must be a scalar on the GPU path")
         nsteps = int(nsteps)
@@ -410,8 +433,10 @@ class PusherGPU:
             rf_omega = rf.omega
             rf_phase = np.array(np.broadcast_to(np.asarray(rf.phase, dtype=np.float64), (m,)))
             rf_phase = torch.from_numpy(rf_phase)
+        surface = self.surface if _collide else None
         tr = DeviceTracker(self.algorithm, self.q_over_m, df, m, nsteps, dt, rec, self.precision,
-                           rf_omega=rf_omega, rf_phase=rf_phase, t0=t0, record=True, device=self.device)
+                           rf_omega=rf_omega, rf_phase=rf_phase, t0=t0, record=True, device=self.device,
+                           surface=surface)
         self.last_tracker = tr
         chunk = self.steps_per_launch or default_steps_per_launch(m, nsteps)
         sort_every = self._sort_interval(m)
@@ -462,7 +487,7 @@ class PusherGPU:
                           "longer exact (use precision='fp64' for such tracks)", RuntimeWarning)
         if verbose:
             print(f"Tracking complete: {nsteps} steps, {m} particles")
-        active = np.ones(m, dtype=bool)
+        active = np.ones(m, dtype=bool) if tr.active is None else tr.active.cpu().numpy().astype(bool)
         if not to_host:
             return tr.r_hist, tr.v_hist, active
         return h_r.numpy(), h_v.numpy(), active
@@ -479,9 +504,10 @@ class PusherGPU:
         snap = self.snapshot
         self.snapshot = "host"
         try:
+            # the reference's single-particle track makes no collision test
             rh, vh, _ = self.track_batch(np.asarray(r0, dtype=np.float64).reshape(1, 3),
                                          np.asarray(v0, dtype=np.float64).reshape(1, 3), efield, bfield,
-                                         nsteps, dt, rec_every_n_steps)
+                                         nsteps, dt, rec_every_n_steps, _collide=False)
         finally:
             self.snapshot = snap
         return rh[:, 0, :], vh[:, 0, :]
@@ -491,6 +517,7 @@ class PusherGPU:
         algorithm = algorithm.lower()
         if algorithm not in self.ALGORITHMS + self.EXTRA_ALGORITHMS:
             raise ValueError(f"Unknown algorithm '{algorithm}'. Must be one of {self.ALGORITHMS}")
+        # as the reference (pusher.py:1033), the electrode assembly is not carried over
         self.__init__(self.ion, algorithm=algorithm, use_numba=self.use_numba, precision=self.precision,
                       device=self.device, snapshot=self.snapshot, steps_per_launch=self.steps_per_launch,
                       sort_every=self.sort_every)

@@ -28,7 +28,7 @@ def test_library_exports_every_header_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(_lib.SIGNATURES)
-    assert lib.ppt_abi_version() == 1
+    assert lib.ppt_abi_version() == 2
 
 
 def test_struct_layouts_match_header():
@@ -36,7 +36,7 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.GridDesc) == 48
     assert ctypes.sizeof(_lib.Fields) == 4 * 8 + 8 + 48
     assert ctypes.sizeof(_lib.State) == 40
-    assert ctypes.sizeof(_lib.TrackArgs) == 4 * 8 + 8 + 4 * 8 + 6 * 8
+    assert ctypes.sizeof(_lib.TrackArgs) == 4 * 8 + 8 + 4 * 8 + 8 * 8
 
 
 def test_capi_argument_errors_without_gpu():
