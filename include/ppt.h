@@ -29,6 +29,8 @@
  *   ppt_surface_*   PyElectrodeAssembly.segment_intersects_surface, the collision
  *                   test track_batch makes each step (pusher.py:982-990; the
  *                   assembly comes from the external py_electrodes package)
+ *   ppt_polar_to_cartesian  the RegularGridInterpolator resampling of the
+ *                   cylindrical-map loaders (field_loaders.py:612-640, :836-899)
  *   ppt_cell_sort   no reference counterpart: particle reordering for gather
  *                   locality (the reference has no particle ordering step)
  */
@@ -223,6 +225,25 @@ typedef struct {
  * later snapshots and the final half step leave its rows untouched
  * (pusher.py:966-1007).  Set active to 1 before the first call. */
 int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_track_args* args, void* stream);
+
+/* ---- cylindrical maps onto a Cartesian grid -------------------------------
+ * The resampling step of the reference's cylindrical-map loaders
+ * (load_opal_midplane, load_aima_agora: field_loaders.py:612-640, :836-899).
+ * r: device nr node radii; theta: device nt node angles [deg]; both increasing. */
+typedef struct {
+    int64_t nr, nt;
+    const double* r;
+    const double* theta;
+} ppt_polar_grid;
+
+/* For every Cartesian node (x[i], y[j]) (device arrays): r = |(x, y)| * r_scale,
+ * theta = atan2(y, x) in degrees, wrapped to [0, 360); (B_r, B_theta, B_z) =
+ * bilinear interpolation of comp[0..2] (device (nr, nt) float64, NULL = zero)
+ * on the polar grid, 0 outside it; out[0] = B_r cos - B_theta sin, out[1] =
+ * B_r sin + B_theta cos, out[2] = B_z: device (nx, ny) float64, NULL = skip. */
+int ppt_polar_to_cartesian(const ppt_polar_grid* grid, const double* const comp[3], int64_t nx,
+                           const double* x, int64_t ny, const double* y, double r_scale,
+                           double* const out[3], void* stream);
 
 /* ---- electrode surfaces -------------------------------------------------
  * Replaces the external PyElectrodeAssembly the reference calls each step

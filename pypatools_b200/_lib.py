@@ -67,6 +67,10 @@ class JobDesc(ctypes.Structure):
 
 
 # name -> (restype, argtypes); every symbol include/ppt.h declares
+class PolarGrid(ctypes.Structure):
+    _fields_ = [("nr", c_int64), ("nt", c_int64), ("r", c_void_p), ("theta", c_void_p)]
+
+
 class MeshDesc(ctypes.Structure):
     _fields_ = [("extent", c_double * 3), ("cells", c_int64 * 3)]
 
@@ -75,6 +79,8 @@ SIGNATURES = {
     "ppt_fieldmap_create": (c_int, [POINTER(GridDesc), c_int, c_int, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_layout": (c_int, [c_uint32]),
     "ppt_deposit_cic": (c_int, [c_int64, c_void_p, c_void_p, POINTER(MeshDesc), c_void_p, c_void_p]),
+    "ppt_polar_to_cartesian": (c_int, [POINTER(PolarGrid), POINTER(c_void_p * 3), c_int64, c_void_p, c_int64,
+                                       c_void_p, c_double, POINTER(c_void_p * 3), c_void_p]),
     "ppt_surface_create": (c_int, [c_int64, c_void_p, c_int64, c_void_p, POINTER(c_void_p)]),
     "ppt_surface_destroy": (c_int, [c_void_p]),
     "ppt_surface_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32)]),

@@ -10,8 +10,12 @@ passes.  As in the reference, a 1D field varies along z and a 2D field along
 x and y (field.py:457-489).
 
 The pusher accepts these objects and the reference's own equally (see
-``device_fields``).  File loaders are not part of this package.
+``device_fields``).  ``Field.from_file`` reads the reference's map formats
+(``loaders``).
 """
+import os
+import pickle
+
 import numpy as np
 
 from . import _lib
@@ -122,8 +126,46 @@ class Field(FieldBase):
 
     @classmethod
     def from_file(cls, filename, **kwargs):
-        raise NotImplementedError("field-map file loaders are not part of the GPU pusher package; "
-                                  "load with the reference and pass its Field object")
+        """Field from a map file, the format chosen by extension (field.py:284-343):
+        .table OPERA, .comsol COMSOL, .dat OPAL midplane, .map AIMA AGORA,
+        .h5/.h5part H5Part, .pickle a saved Field.  As in the reference,
+        ``kwargs`` go to the constructor, not to the loader."""
+        from . import loaders
+        if not os.path.exists(filename):
+            raise FileNotFoundError(f"Field file not found: {filename}")
+        ext = os.path.splitext(filename)[1]
+        field = cls(**kwargs)
+        field._filename = filename
+        if ext == ".pickle":
+            field._load_pickle(filename)
+            return field
+        if ext not in loaders.LOADERS:
+            raise ValueError(f"Unknown file extension: {ext}")
+        data = loaders.LOADERS[ext](filename)
+        points = [data["grid"][k] for k in "xyz" if k in data["grid"] and len(data["grid"][k]) > 1]
+        field._dim = data["dim"]
+        field._metadata = data["metadata"]
+        for c in "xyz":
+            if c in data["values"]:
+                field._field[c] = get_interpolator(tuple(points), data["values"][c], method=field._method,
+                                                   bounds_error=False, fill_value=0.0,
+                                                   backend=field._interpolator_backend)
+        return field
+
+    def _load_pickle(self, filename):
+        """Restore a Field saved by ``save_pickle`` (field.py:510-518)."""
+        with open(filename, "rb") as fh:
+            data = pickle.load(fh)
+        for key in ("_label", "_dim", "_scaling", "_field", "_unit_scale", "_metadata"):
+            if key in data:
+                setattr(self, key, data[key])
+
+    def save_pickle(self, filename):
+        """Save the Field's attributes (field.py:520-534)."""
+        data = {"_label": self._label, "_dim": self._dim, "_scaling": self._scaling, "_field": self._field,
+                "_unit_scale": self._unit_scale, "_metadata": self._metadata}
+        with open(filename, "wb") as fh:
+            pickle.dump(data, fh)
 
     @classmethod
     def zero(cls, dim=3):

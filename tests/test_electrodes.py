@@ -143,12 +143,12 @@ def _compare(got, ref, hw):
 @pytest.mark.parametrize("alg", ["boris", "rk4_rel", "vay_rel", "leapfrog"])
 def test_gpu_track_with_surface_matches_oracle(cuda, alg):
     from pypatools_b200 import PusherGPU
-    wl = workloads.quad_solenoid_protons(n=512, nsteps=600, rec_every=50)
+    wl = workloads.quad_solenoid_protons(n=192, nsteps=400, rec_every=50)
     e, b = gpu_fields(wl)
     oe, ob = oracle_fields(wl)
     s = _beamline()
-    got = PusherGPU(wl.species, alg, electrode_assembly=s).track_batch(wl.r0, wl.v0, e, b, 600, wl.dt, 50)
-    ref = orc.track_batch(alg, wl.species.q_over_m, wl.r0, wl.v0, oe, ob, 600, wl.dt, 50,
+    got = PusherGPU(wl.species, alg, electrode_assembly=s).track_batch(wl.r0, wl.v0, e, b, 400, wl.dt, 50)
+    ref = orc.track_batch(alg, wl.species.q_over_m, wl.r0, wl.v0, oe, ob, 400, wl.dt, 50,
                           surface=(s.vertices, s.triangles))
     assert 0 < ref[2].sum() < ref[2].size
     _compare(got, ref, half_width(wl))
