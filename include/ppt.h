@@ -26,6 +26,8 @@
  *                   693-719, :761-788, :507-525, :393-457)
  *   ppt_deposit_cic PyAMGPoissonSolver's CIC charge deposition
  *                   (src/PyPATools/poisson_amg.py:849-911)
+ *   ppt_poisson_*, ppt_field_from_potential  PyAMGPoissonSolver.solve's
+ *                   linear solve and E = -grad phi (poisson_amg.py:616-797)
  *   ppt_surface_*   PyElectrodeAssembly.segment_intersects_surface, the collision
  *                   test track_batch makes each step (pusher.py:982-990; the
  *                   assembly comes from the external py_electrodes package)
@@ -333,6 +335,23 @@ typedef struct {
  * Float64 atomics: results agree with the sequential sum to rounding. */
 int ppt_deposit_cic(int64_t n, const double* r, const double* q, const ppt_mesh_desc* mesh, double* rho,
                     void* stream);
+
+/* ---- space charge: the potential and field on the solver's mesh ----------
+ * PyAMGPoissonSolver's linear solve and field step for a domain without
+ * conductor cells (src/PyPATools/poisson_amg.py:616-797; operator :293-443,
+ * rhs = rho / eps0 :913-921, E = -grad phi :98-130).  The mesh has cells[a]
+ * cells of size extent[a] / cells[a] centred at -extent/2 + (i + 1/2) h;
+ * rhs, phi, ex, ey, ez are device (nx, ny, nz) float64 arrays.
+ * ppt_poisson_solve: conjugate gradients, matrix-free, from the initial guess
+ * in phi until |r| <= rel_tol |rhs| or max_iter iterations; synchronises the
+ * stream a few times; reports the iterations and the final |r| / |rhs|.
+ * ppt_field_from_potential: central differences at cells whose three indices
+ * are interior, 0 on the outer layer (any of ex, ey, ez may be NULL). */
+int64_t ppt_poisson_scratch_bytes(const ppt_mesh_desc* mesh);
+int ppt_poisson_solve(const ppt_mesh_desc* mesh, const double* rhs, double* phi, void* scratch, double rel_tol,
+                      int64_t max_iter, int64_t* iterations, double* rel_residual, void* stream);
+int ppt_field_from_potential(const ppt_mesh_desc* mesh, const double* phi, double* ex, double* ey, double* ez,
+                             void* stream);
 
 /* Bunch moments of n particles from (n,3) float64 positions and velocities
  * (device), in float64:

@@ -81,6 +81,10 @@ SIGNATURES = {
     "ppt_deposit_cic": (c_int, [c_int64, c_void_p, c_void_p, POINTER(MeshDesc), c_void_p, c_void_p]),
     "ppt_polar_to_cartesian": (c_int, [POINTER(PolarGrid), POINTER(c_void_p * 3), c_int64, c_void_p, c_int64,
                                        c_void_p, c_double, POINTER(c_void_p * 3), c_void_p]),
+    "ppt_poisson_scratch_bytes": (c_int64, [POINTER(MeshDesc)]),
+    "ppt_poisson_solve": (c_int, [POINTER(MeshDesc), c_void_p, c_void_p, c_void_p, c_double, c_int64,
+                                  POINTER(c_int64), POINTER(c_double), c_void_p]),
+    "ppt_field_from_potential": (c_int, [POINTER(MeshDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_surface_create": (c_int, [c_int64, c_void_p, c_int64, c_void_p, POINTER(c_void_p)]),
     "ppt_surface_destroy": (c_int, [c_void_p]),
     "ppt_surface_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32)]),

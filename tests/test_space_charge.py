@@ -1,0 +1,131 @@
+"""Space-charge solve: deposition, Poisson solve and E = -grad phi
+(PyAMGPoissonSolver, src/PyPATools/poisson_amg.py) for a domain without
+conductor cells.
+
+The oracle's operator and field step are pinned bit for bit to the
+reference's own matrix assembly and field function (tests/golden/
+poisson_golden.npz, made by make_golden_poisson.py).  The GPU solve is held to
+the exact solution of that operator (sparse direct solve) at 1e-8 relative
+when solved to a 1e-12 residual; the field step to the reference bit for bit."""
+import ctypes
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import space_charge_oracle as sco
+from pypatools_b200 import _lib
+from tests.conftest import REPO
+
+G = np.load(REPO / "tests" / "golden" / "poisson_golden.npz")
+CASES = ("box", "flat")
+
+
+def _mesh(extent, cells):
+    m = _lib.MeshDesc()
+    for a in range(3):
+        m.extent[a] = extent[a]
+        m.cells[a] = int(cells[a])
+    return m
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_operator_matches_reference_bitwise(name):
+    cells = tuple(int(c) for c in G[f"{name}/cells"])
+    m = int(np.prod(cells))
+    ref = sp.csr_matrix((G[f"{name}/A_val"], (G[f"{name}/A_row"], G[f"{name}/A_col"])), shape=(m, m))
+    ours = sco.assemble_matrix(G[f"{name}/extent"], cells)
+    assert (ours != ref).nnz == 0
+    np.testing.assert_array_equal(ours.toarray(), ref.toarray())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_field_matches_reference_bitwise(name):
+    ex, ey, ez = sco.field_from_potential(G[f"{name}/phi"], G[f"{name}/extent"])
+    for got, key in ((ex, "ex"), (ey, "ey"), (ez, "ez")):
+        np.testing.assert_array_equal(got, G[f"{name}/{key}"])
+
+
+def test_poisson_argument_checks_without_gpu():
+    lib = _lib.load()
+    assert lib.ppt_poisson_scratch_bytes(None) == -1
+    mesh = _mesh((0.1, 0.1, 0.1), (4, 4, 4))
+    m, nb = 64, 1
+    assert lib.ppt_poisson_scratch_bytes(mesh) == (3 * m + 2 * nb + 7) * 8
+    it, res = ctypes.c_int64(), ctypes.c_double()
+    assert lib.ppt_poisson_solve(mesh, None, None, None, 1e-6, 10, it, res, None) == -1
+    bad = _mesh((0.1, -1.0, 0.1), (4, 4, 4))
+    assert lib.ppt_field_from_potential(bad, ctypes.c_void_p(16), None, None, None, None) == -1
+    assert b"positive" in lib.ppt_last_error()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_gpu_field_from_potential_matches_reference_bitwise(cuda, name):
+    torch = cuda
+    phi = torch.from_numpy(G[f"{name}/phi"]).cuda()
+    e = torch.empty((3,) + tuple(phi.shape), dtype=torch.float64, device="cuda")
+    _lib.check(_lib.load().ppt_field_from_potential(_mesh(G[f"{name}/extent"], phi.shape), phi.data_ptr(),
+                                                    e[0].data_ptr(), e[1].data_ptr(), e[2].data_ptr(),
+                                                    _lib.stream_handle()))
+    e = e.cpu().numpy()
+    for k, key in enumerate(("ex", "ey", "ez")):
+        np.testing.assert_array_equal(e[k], G[f"{name}/{key}"])
+
+
+@pytest.mark.gpu
+def test_gpu_poisson_solve_vs_direct_solve(cuda):
+    torch = cuda
+    extent, cells = (0.1, 0.08, 0.16), (24, 20, 28)
+    rng = np.random.default_rng(7)
+    b = rng.normal(0, 1.0, cells)
+    exact = sco.spsolve(sco.assemble_matrix(extent, cells).tocsc(), b.ravel()).reshape(cells)
+    lib = _lib.load()
+    mesh = _mesh(extent, cells)
+    scratch = torch.empty(lib.ppt_poisson_scratch_bytes(mesh), dtype=torch.uint8, device="cuda")
+    d_b = torch.from_numpy(b).cuda()
+    outs = []
+    for _ in range(2):
+        phi = torch.zeros(cells, dtype=torch.float64, device="cuda")
+        it, res = ctypes.c_int64(), ctypes.c_double()
+        _lib.check(lib.ppt_poisson_solve(mesh, d_b.data_ptr(), phi.data_ptr(), scratch.data_ptr(), 1e-12, 5000,
+                                         it, res, _lib.stream_handle()))
+        assert 0 < it.value < 5000 and res.value <= 1e-12
+        outs.append(phi.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])            # deterministic
+    err = np.abs(outs[0] - exact).max() / np.abs(exact).max()
+    assert err < 1e-8, err
+    # the residual the solver reports is the true one
+    a = sco.assemble_matrix(extent, cells)
+    true_res = np.linalg.norm(a @ outs[0].ravel() - b.ravel()) / np.linalg.norm(b)
+    assert true_res < 1e-11
+
+
+@pytest.mark.gpu
+def test_gpu_space_charge_solve_vs_oracle(cuda):
+    from pypatools_b200.space_charge import PoissonSolverConfig, SpaceChargeSolver
+    rng = np.random.default_rng(8)
+    extent, cells = (0.04, 0.04, 0.1), (16, 16, 32)
+    n = 50_000
+    p = np.column_stack([rng.normal(0, 3e-3, n), rng.normal(0, 3e-3, n), rng.normal(0, 1e-2, n)])
+    q = np.full(n, 1.602176634e-19 * 1e4)
+    solver = SpaceChargeSolver(PoissonSolverConfig(extent, cells, solver_tol=1e-12))
+    phi, field = solver.solve(p, q)
+    ref = sco.solve(p, q, extent, cells)
+    scale = np.abs(ref[0]).max()
+    np.testing.assert_allclose(phi, ref[0], rtol=0, atol=1e-8 * scale)
+    e = solver.e.cpu().numpy()
+    for k in range(3):
+        np.testing.assert_allclose(e[k], ref[k + 1], rtol=0, atol=1e-8 * np.abs(ref[k + 1]).max())
+    # the returned Field interpolates the field on the cell centres
+    assert field.dim == 3 and solver.turn_count == 1
+    pts = np.column_stack([rng.uniform(-0.015, 0.015, 500), rng.uniform(-0.015, 0.015, 500),
+                           rng.uniform(-0.04, 0.04, 500)])
+    from oracle import pusher_oracle as orc
+    oe = orc.MapField(solver.cell_centres(), {"x": ref[1], "y": ref[2], "z": ref[3]})(pts)
+    np.testing.assert_allclose(field(pts), oe, rtol=0, atol=1e-8 * np.abs(oe).max())
+    # no charge: zero potential, no iterations
+    phi0, _ = solver.solve(np.zeros((0, 3)), np.zeros(0))
+    assert not np.any(phi0) and solver.last_iterations == 0
+    with pytest.raises(NotImplementedError):
+        SpaceChargeSolver(PoissonSolverConfig(extent, cells), electrode_assembly=object())
