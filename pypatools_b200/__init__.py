@@ -15,7 +15,8 @@ from .particles import ParticleDistribution
 from .moments import bunch_moments
 from .deposit import bin_particles_cic
 from .electrodes import ElectrodeSurface
+from .beam import Beam
 
 __all__ = ["IonSpecies", "PRESETS", "Field", "ScaledField", "CompositeField", "FieldMap", "get_interpolator",
            "CudaInterpolator", "Pusher", "PusherGPU", "RFModulation", "DeviceTracker", "ParticleDistribution",
-           "bunch_moments", "bin_particles_cic", "ElectrodeSurface"]
+           "bunch_moments", "bin_particles_cic", "ElectrodeSurface", "Beam"]
