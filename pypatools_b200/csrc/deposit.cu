@@ -36,18 +36,40 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// One particle's position and charge (a particle past n reads nothing).
+struct Loaded {
+    double x[3];
+    double q;
+    bool in;
+};
+
+__device__ __forceinline__ Loaded load_particle(int64_t s, int64_t n, const double* __restrict__ r,
+                                                const double* __restrict__ q) {
+    Loaded L;
+    L.in = s < n;
+    if (L.in) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) L.x[a] = r[3 * s + a];
+        L.q = q[s];
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) L.x[a] = 0.0;
+        L.q = 0.0;
+    }
+    return L;
+}
+
 // One particle's cell (linear index of its lower corner) and corner charges;
 // an invalid particle (past n, or a NaN position) gets cell -1 and no charge.
-__device__ __forceinline__ int64_t particle_corners(int64_t s, int64_t n, const double* __restrict__ r,
-                                                    const double* __restrict__ q, const MeshGeom& G,
-                                                    const int64_t strides[3], double w[8]) {
-    bool valid = s < n;
+__device__ __forceinline__ int64_t particle_corners(const Loaded& L, const MeshGeom& G, const int64_t strides[3],
+                                                    double w[8]) {
+    bool valid = L.in;
     int64_t idx[3] = {0, 0, 0};
     double f[3] = {0.0, 0.0, 0.0};
     if (valid) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            double p = (r[3 * s + a] + G.half[a]) / G.h[a];
+            double p = (L.x[a] + G.half[a]) / G.h[a];
             valid = valid && !isnan(p);                        // a NaN position deposits nothing
             const double top = (double)(G.n[a] - 1);
             p = p < 0.0 ? 0.0 : (p > top ? top : p);          // np.clip
@@ -59,7 +81,7 @@ __device__ __forceinline__ int64_t particle_corners(int64_t s, int64_t n, const 
             idx[a] = (int64_t)i;
         }
     }
-    const double qs = valid ? q[s] : 0.0;
+    const double qs = valid ? L.q : 0.0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const int di = (c >> 2) & 1, dj = (c >> 1) & 1, dk = c & 1;
@@ -85,7 +107,8 @@ __device__ __forceinline__ void add_corners(double* rho, int64_t base, const int
 // the cell changes (or at the end) the warp reduces them with shuffles and
 // lane 0 issues 8 atomics.  A round whose particles are not all in one cell
 // adds per lane.  A cell-sorted bunch thus costs 8 atomics per cell and warp
-// instead of 8 per particle.
+// instead of 8 per particle.  The next round's particle is loaded before the
+// current one is processed, so its memory latency overlaps the arithmetic.
 constexpr int kRounds = 8;
 
 __global__ void __launch_bounds__(256) deposit_cic_kernel(int64_t n, const double* __restrict__ r,
@@ -99,11 +122,13 @@ __global__ void __launch_bounds__(256) deposit_cic_kernel(int64_t n, const doubl
     double acc[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+    Loaded next = load_particle(first + lane, n, r, q);
     for (int round = 0; round < kRounds; ++round) {
-        const int64_t s = first + round * 32 + lane;
         if (first + round * 32 >= n) break;          // warp-uniform
+        const Loaded part = next;
+        if (round + 1 < kRounds) next = load_particle(first + (round + 1) * 32 + lane, n, r, q);
         double w[8];
-        const int64_t base = particle_corners(s, n, r, q, G, strides, w);
+        const int64_t base = particle_corners(part, G, strides, w);
         const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)base);
         const bool uniform = peers == 0xffffffffu && base >= 0;   // the same for every lane
         if (uniform && base == cur) {
