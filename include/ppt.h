@@ -267,6 +267,17 @@ int ppt_surface_info(const ppt_surface* surface, int64_t* bytes, int32_t dims[3]
 int ppt_surface_segments_hit(const ppt_surface* surface, int64_t n, const double* p0, const double* p1,
                              uint8_t* hit, void* stream);
 
+/* For each point and each direction d = +x, -x, +y, -y, +z, -z (in that
+ * order): hits[6 i + d] = the number of triangles the ray from the point
+ * along d crosses (Moller-Trumbore, t >= 0), min_dist[6 i + d] = the distance
+ * to the nearest of them (INFINITY without any).  The axis-aligned ray casting
+ * the reference's solver asks of its electrode assembly to classify mesh
+ * cells (compute_axis_aligned_surface_intersections, poisson_amg.py:249-251).
+ * points: device (n,3) float64; min_dist: device (n,6) float64; hits: device
+ * (n,6) int32. */
+int ppt_surface_axis_rays(const ppt_surface* surface, int64_t n, const double* points, double* min_dist,
+                          int32_t* hits, void* stream);
+
 /* ---- serving: many jobs per launch -------------------------------------
  * No reference counterpart (the reference runs one track_batch at a time,
  * pusher.py:894-1012).  A job is one track_batch call's device state. */
@@ -352,6 +363,17 @@ int ppt_poisson_solve(const ppt_mesh_desc* mesh, const double* rhs, double* phi,
                       int64_t max_iter, int64_t* iterations, double* rel_residual, void* stream);
 int ppt_field_from_potential(const ppt_mesh_desc* mesh, const double* phi, double* ex, double* ey, double* ez,
                              void* stream);
+
+/* The same solve with per-cell coefficients, for a domain with conductor
+ * cells (the reference's Shortley-Weller rows, poisson_amg.py:293-443):
+ * coef: device (nx*ny*nz, 7) float64 = diagonal and the +x, -x, +y, -y, +z,
+ * -z couplings of each cell's row (0 for a neighbour outside the box or in a
+ * conductor; a conductor cell's row is the identity, its rhs 0).  The
+ * operator is not symmetric: BiCGSTAB.  Scratch: ppt_poisson_coef_scratch_bytes. */
+int64_t ppt_poisson_coef_scratch_bytes(const ppt_mesh_desc* mesh);
+int ppt_poisson_solve_coef(const ppt_mesh_desc* mesh, const double* coef, const double* rhs, double* phi,
+                           void* scratch, double rel_tol, int64_t max_iter, int64_t* iterations,
+                           double* rel_residual, void* stream);
 
 /* Bunch moments of n particles from (n,3) float64 positions and velocities
  * (device), in float64:

@@ -67,3 +67,96 @@ def solve(particles, charges, extent, cells, iterative_tol=None):
         x, _ = cg(a, b, rtol=iterative_tol, atol=0.0, maxiter=20 * max(cells))
     phi = x.reshape([int(c) for c in cells])
     return (phi,) + field_from_potential(phi, extent)
+
+
+# ---------------------------------------------------------------------------
+# Conductor cells (poisson_amg.py:241-443)
+# ---------------------------------------------------------------------------
+
+INTERIOR, BOUNDARY, CONDUCTOR = 0, 1, 2     # CellType (poisson_amg.py:86-90)
+
+
+def axis_ray_hits(points, vertices, triangles):
+    """(min_dist (n,6), hits (n,6)) of the rays from each point along +x, -x,
+    +y, -y, +z, -z: crossings counted over every triangle (Moller-Trumbore,
+    t >= 0, each product and sum rounded separately), distance to the nearest."""
+    p = np.asarray(points, dtype=np.float64).reshape(-1, 3)
+    v = np.asarray(vertices, dtype=np.float64)
+    t = np.asarray(triangles, dtype=np.int64)
+    v0 = v[t[:, 0]]
+    e1 = v[t[:, 1]] - v0
+    e2 = v[t[:, 2]] - v0
+    dist = np.full((p.shape[0], 6), np.inf)
+    hits = np.zeros((p.shape[0], 6), dtype=np.int32)
+
+    def cross(a, b):
+        return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                         a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                         a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1)
+
+    def dot(a, b):
+        return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
+
+    for direction in range(6):
+        d = np.zeros(3)
+        d[direction // 2] = -1.0 if direction % 2 else 1.0
+        pv = cross(d[None, :], e2)                        # per triangle
+        det = dot(e1, pv)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            inv = 1.0 / det
+            for s in range(0, p.shape[0], 2048):
+                tv = p[s:s + 2048, None, :] - v0[None]
+                u = dot(tv, pv[None]) * inv[None]
+                qv = cross(tv, e1[None])
+                w = dot(d[None, None, :], qv) * inv[None]
+                tt = dot(e2[None], qv) * inv[None]
+                ok = (det != 0.0)[None] & (u >= 0.0) & (u <= 1.0) & (w >= 0.0) & (u + w <= 1.0) & (tt >= 0.0)
+                hits[s:s + 2048, direction] = ok.sum(axis=1)
+                dist[s:s + 2048, direction] = np.where(ok, tt, np.inf).min(axis=1)
+    return dist, hits
+
+
+def classify_cells(min_dist, hits, h):
+    """Cell types (poisson_amg.py:258-281): a conductor where a ray crosses the
+    surface an odd number of times in any direction; a boundary cell where a
+    crossing is within one cell size (compared with the sizes as float32)."""
+    is_cond = (hits % 2 != 0).any(axis=1)
+    sizes = np.array([h[0], h[0], h[1], h[1], h[2], h[2]], dtype=np.float32)
+    is_bnd = (min_dist <= sizes).any(axis=1) & ~is_cond
+    out = np.full(hits.shape[0], INTERIOR, dtype=np.int32)
+    out[is_bnd] = BOUNDARY
+    out[is_cond] = CONDUCTOR
+    return out
+
+
+def assemble_reduced(extent, cells, cell_type, dist):
+    """(A, keep): the reference's reduced system over the non-conductor cells,
+    row by row as its assembly loop writes them (Shortley-Weller distances
+    towards conductor neighbours, at least h / 1000)."""
+    n = [int(c) for c in cells]
+    h = [float(e) / c for e, c in zip(extent, n)]
+    m = n[0] * n[1] * n[2]
+    keep = np.nonzero(cell_type != CONDUCTOR)[0]
+    new = np.full(m, -1, dtype=np.int64)
+    new[keep] = np.arange(keep.size)
+    strides = (n[1] * n[2], n[2], 1)
+    rows, cols, vals = [], [], []
+    for c in keep:
+        ijk = (c // strides[0], (c // strides[1]) % n[1], c % n[2])
+        diag = 0.0
+        for a in range(3):
+            has_pos, has_neg = ijk[a] + 1 < n[a], ijk[a] > 0
+            pos, neg = c + strides[a], c - strides[a]
+            cond_pos = has_pos and cell_type[pos] == CONDUCTOR
+            cond_neg = has_neg and cell_type[neg] == CONDUCTOR
+            hp = max(dist[c, 2 * a], h[a] * 1e-3) if cond_pos else h[a]
+            hn = max(dist[c, 2 * a + 1], h[a] * 1e-3) if cond_neg else h[a]
+            diag += 2.0 / (hp * hn)
+            if has_pos and not cond_pos:
+                rows.append(new[c]); cols.append(new[pos]); vals.append(-2.0 / (hp * (hp + hn)))
+            if has_neg and not cond_neg:
+                rows.append(new[c]); cols.append(new[neg]); vals.append(-2.0 / (hn * (hp + hn)))
+        rows.append(new[c]); cols.append(new[c]); vals.append(diag)
+    a = sp.csr_matrix((vals, (rows, cols)), shape=(keep.size, keep.size))
+    a.eliminate_zeros()
+    return a, keep

@@ -84,10 +84,14 @@ SIGNATURES = {
     "ppt_poisson_scratch_bytes": (c_int64, [POINTER(MeshDesc)]),
     "ppt_poisson_solve": (c_int, [POINTER(MeshDesc), c_void_p, c_void_p, c_void_p, c_double, c_int64,
                                   POINTER(c_int64), POINTER(c_double), c_void_p]),
+    "ppt_poisson_coef_scratch_bytes": (c_int64, [POINTER(MeshDesc)]),
+    "ppt_poisson_solve_coef": (c_int, [POINTER(MeshDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_double,
+                                       c_int64, POINTER(c_int64), POINTER(c_double), c_void_p]),
     "ppt_field_from_potential": (c_int, [POINTER(MeshDesc), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_surface_create": (c_int, [c_int64, c_void_p, c_int64, c_void_p, POINTER(c_void_p)]),
     "ppt_surface_destroy": (c_int, [c_void_p]),
     "ppt_surface_info": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32)]),
+    "ppt_surface_axis_rays": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_surface_segments_hit": (c_int, [c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_fieldmap_create_masked": (c_int, [POINTER(GridDesc), c_uint32, c_int, POINTER(c_void_p)]),
     "ppt_fieldmap_add": (c_int, [c_void_p, POINTER(c_void_p * 6), POINTER(c_double * 6), c_int, c_void_p]),

@@ -194,6 +194,153 @@ __global__ void __launch_bounds__(kBlock) field_from_potential(int64_t nx, int64
     if (ez) ez[c] = fz;
 }
 
+// ---------------------------------------------------------------------------
+// Operator with per-cell coefficients (conductor cells, Shortley-Weller rows):
+// coef[7 c .. 7 c + 6] = diagonal, +x, -x, +y, -y, +z, -z couplings (0 for a
+// neighbour outside the box or in a conductor; a conductor cell's row is the
+// identity).  Not symmetric in general: BiCGSTAB (H. A. van der Vorst, SIAM J.
+// Sci. Stat. Comput. 13(2), 1992).
+// ---------------------------------------------------------------------------
+struct CoefOp {
+    int64_t n[3];
+    const double* coef;
+};
+
+enum { bRR = 0, bBB, bTOL2, bRHO, bALPHA, bOMEGA, bBETA, bDONE, bITERS, bNumScalars };
+
+__device__ __forceinline__ double apply_coef(const CoefOp& A, const double* __restrict__ x, int64_t c) {
+    const int64_t nz = A.n[2], sy = nz, sx = A.n[1] * nz;
+    const int64_t k = c % nz, t = c / nz, j = t % A.n[1], i = t / A.n[1];
+    const double* w = A.coef + 7 * c;
+    double s = w[0] * x[c];
+    if (i + 1 < A.n[0]) s += w[1] * x[c + sx];
+    if (i > 0) s += w[2] * x[c - sx];
+    if (j + 1 < A.n[1]) s += w[3] * x[c + sy];
+    if (j > 0) s += w[4] * x[c - sy];
+    if (k + 1 < A.n[2]) s += w[5] * x[c + 1];
+    if (k > 0) s += w[6] * x[c - 1];
+    return s;
+}
+
+// r = b - A x, rhat = r, p = v = 0; partial sums of r.r and b.b
+__global__ void __launch_bounds__(kBlock) bi_start(const __grid_constant__ CoefOp A, int64_t m,
+                                                   const double* __restrict__ b, const double* __restrict__ x,
+                                                   double* __restrict__ r, double* __restrict__ rhat,
+                                                   double* __restrict__ p, double* __restrict__ v,
+                                                   double* __restrict__ part, double* __restrict__ part2) {
+    const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+    double rr = 0.0, bb = 0.0;
+    if (c < m) {
+        const double rc = b[c] - apply_coef(A, x, c);
+        r[c] = rc;
+        rhat[c] = rc;
+        p[c] = 0.0;
+        v[c] = 0.0;
+        rr = rc * rc;
+        bb = b[c] * b[c];
+    }
+    block_partial(rr, part);
+    __syncthreads();
+    block_partial(bb, part2);
+}
+
+// p = r + beta (p - omega v)
+__global__ void __launch_bounds__(kBlock) bi_direction(int64_t m, const double* __restrict__ r, double* __restrict__ p,
+                                                       const double* __restrict__ v, const double* __restrict__ S) {
+    if (S[bDONE] != 0.0) return;
+    const double beta = S[bBETA], omega = S[bOMEGA];
+    const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+    if (c < m) p[c] = r[c] + beta * (p[c] - omega * v[c]);
+}
+
+// y = A z; partial sums of a.y (and of y.y when part2 is set)
+__global__ void __launch_bounds__(kBlock) bi_apply(const __grid_constant__ CoefOp A, int64_t m,
+                                                   const double* __restrict__ z, double* __restrict__ y,
+                                                   const double* __restrict__ a, double* __restrict__ part,
+                                                   double* __restrict__ part2, const double* __restrict__ S) {
+    if (S[bDONE] != 0.0) return;
+    const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+    double d1 = 0.0, d2 = 0.0;
+    if (c < m) {
+        const double yc = apply_coef(A, z, c);
+        y[c] = yc;
+        d1 = a[c] * yc;
+        d2 = yc * yc;
+    }
+    block_partial(d1, part);
+    if (part2) {
+        __syncthreads();
+        block_partial(d2, part2);
+    }
+}
+
+// s = r - alpha v
+__global__ void __launch_bounds__(kBlock) bi_half(int64_t m, const double* __restrict__ r, const double* __restrict__ v,
+                                                  double* __restrict__ sv, const double* __restrict__ S) {
+    if (S[bDONE] != 0.0) return;
+    const double alpha = S[bALPHA];
+    const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+    if (c < m) sv[c] = r[c] - alpha * v[c];
+}
+
+// x += alpha p + omega s, r = s - omega t; partial sums of rhat.r and r.r
+__global__ void __launch_bounds__(kBlock) bi_update(int64_t m, double* __restrict__ x, double* __restrict__ r,
+                                                    const double* __restrict__ rhat, const double* __restrict__ p,
+                                                    const double* __restrict__ sv, const double* __restrict__ t,
+                                                    double* __restrict__ part, double* __restrict__ part2,
+                                                    const double* __restrict__ S) {
+    if (S[bDONE] != 0.0) return;
+    const double alpha = S[bALPHA], omega = S[bOMEGA];
+    const int64_t c = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+    double d1 = 0.0, d2 = 0.0;
+    if (c < m) {
+        x[c] += alpha * p[c] + omega * sv[c];
+        const double rc = sv[c] - omega * t[c];
+        r[c] = rc;
+        d1 = rhat[c] * rc;
+        d2 = rc * rc;
+    }
+    block_partial(d1, part);
+    __syncthreads();
+    block_partial(d2, part2);
+}
+
+// One block.  mode 0: start; 1: alpha = rho / rhat.v; 2: omega = t.s / t.t;
+// 3: rho', beta, residual and the stopping test.
+__global__ void __launch_bounds__(kBlock) bi_scalars(int mode, const double* __restrict__ part,
+                                                     const double* __restrict__ part2, int nb, double* S,
+                                                     double rel_tol, int64_t max_iter) {
+    if (mode != 0 && S[bDONE] != 0.0) return;
+    const double a = sum_partials(part, nb);
+    __syncthreads();
+    const double b = part2 ? sum_partials(part2, nb) : 0.0;
+    if (threadIdx.x != 0) return;
+    if (mode == 0) {
+        S[bRR] = a;
+        S[bBB] = b;
+        S[bTOL2] = rel_tol * rel_tol * b;
+        S[bRHO] = a;          // rhat = r
+        S[bALPHA] = 1.0;
+        S[bOMEGA] = 1.0;
+        S[bBETA] = 0.0;       // first direction p = r
+        S[bITERS] = 0.0;
+        S[bDONE] = (a <= S[bTOL2] || a == 0.0 || max_iter <= 0) ? 1.0 : 0.0;
+    } else if (mode == 1) {
+        S[bALPHA] = a != 0.0 ? S[bRHO] / a : 0.0;
+        if (a == 0.0) S[bDONE] = 1.0;                       // breakdown
+    } else if (mode == 2) {
+        S[bOMEGA] = b > 0.0 ? a / b : 0.0;                  // a = t.s, b = t.t
+    } else {
+        S[bITERS] += 1.0;
+        S[bRR] = b;
+        const double rho = a;
+        S[bBETA] = (S[bRHO] != 0.0 && S[bOMEGA] != 0.0) ? (rho / S[bRHO]) * (S[bALPHA] / S[bOMEGA]) : 0.0;
+        S[bRHO] = rho;
+        if (b <= S[bTOL2] || b == 0.0 || S[bITERS] >= (double)max_iter || rho == 0.0 || S[bOMEGA] == 0.0)
+            S[bDONE] = 1.0;
+    }
+}
+
 static int mesh_geom(const ppt_mesh_desc* mesh, int64_t n[3], double h[3]) {
     if (!mesh) return fail(PPT_ERR_ARG, "mesh must not be NULL");
     int64_t total = 1;
@@ -284,5 +431,66 @@ extern "C" int ppt_field_from_potential(const ppt_mesh_desc* mesh, const double*
     field_from_potential<<<(unsigned)((m + kBlock - 1) / kBlock), kBlock, 0, static_cast<cudaStream_t>(stream)>>>(
         n[0], n[1], n[2], phi, h[0], h[1], h[2], ex, ey, ez);
     PPT_CUDA_TRY(cudaGetLastError());
+    return PPT_OK;
+}
+
+extern "C" int64_t ppt_poisson_coef_scratch_bytes(const ppt_mesh_desc* mesh) {
+    int64_t n[3];
+    double h[3];
+    if (mesh_geom(mesh, n, h)) return -1;
+    const int64_t m = n[0] * n[1] * n[2];
+    const int64_t nb = (m + kBlock - 1) / kBlock;
+    return (6 * m + 2 * nb + bNumScalars) * (int64_t)sizeof(double);
+}
+
+extern "C" int ppt_poisson_solve_coef(const ppt_mesh_desc* mesh, const double* coef, const double* rhs, double* phi,
+                                      void* scratch, double rel_tol, int64_t max_iter, int64_t* iterations,
+                                      double* rel_residual, void* stream) {
+    int64_t n[3];
+    double h[3];
+    int rc = mesh_geom(mesh, n, h);
+    if (rc) return rc;
+    if (!coef || !rhs || !phi || !scratch) return fail(PPT_ERR_ARG, "coef, rhs, phi and scratch must not be NULL");
+    if (!(rel_tol >= 0.0)) return fail(PPT_ERR_ARG, "rel_tol must be >= 0");
+    CoefOp A;
+    for (int a = 0; a < 3; ++a) A.n[a] = n[a];
+    A.coef = coef;
+    const int64_t m = n[0] * n[1] * n[2];
+    const int nb = (int)((m + kBlock - 1) / kBlock);
+    double* r = static_cast<double*>(scratch);
+    double* rhat = r + m;
+    double* p = rhat + m;
+    double* v = p + m;
+    double* sv = v + m;
+    double* t = sv + m;
+    double* part = t + m;
+    double* part2 = part + nb;
+    double* S = part2 + nb;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    bi_start<<<nb, kBlock, 0, st>>>(A, m, rhs, phi, r, rhat, p, v, part, part2);
+    bi_scalars<<<1, kBlock, 0, st>>>(0, part, part2, nb, S, rel_tol, max_iter);
+    PPT_CUDA_TRY(cudaGetLastError());
+    double host[bNumScalars];
+    int64_t batch = 8;
+    for (int64_t done = 0;;) {
+        for (int64_t it = 0; it < batch; ++it) {
+            bi_direction<<<nb, kBlock, 0, st>>>(m, r, p, v, S);
+            bi_apply<<<nb, kBlock, 0, st>>>(A, m, p, v, rhat, part, nullptr, S);
+            bi_scalars<<<1, kBlock, 0, st>>>(1, part, nullptr, nb, S, rel_tol, max_iter);
+            bi_half<<<nb, kBlock, 0, st>>>(m, r, v, sv, S);
+            bi_apply<<<nb, kBlock, 0, st>>>(A, m, sv, t, sv, part, part2, S);
+            bi_scalars<<<1, kBlock, 0, st>>>(2, part, part2, nb, S, rel_tol, max_iter);
+            bi_update<<<nb, kBlock, 0, st>>>(m, phi, r, rhat, p, sv, t, part, part2, S);
+            bi_scalars<<<1, kBlock, 0, st>>>(3, part, part2, nb, S, rel_tol, max_iter);
+        }
+        PPT_CUDA_TRY(cudaGetLastError());
+        done += batch;
+        PPT_CUDA_TRY(cudaMemcpyAsync(host, S, sizeof(host), cudaMemcpyDeviceToHost, st));
+        PPT_CUDA_TRY(cudaStreamSynchronize(st));
+        if (host[bDONE] != 0.0 || done >= max_iter) break;
+        batch = batch < 64 ? batch * 2 : 64;
+    }
+    if (iterations) *iterations = (int64_t)host[bITERS];
+    if (rel_residual) *rel_residual = host[bBB] > 0.0 ? std::sqrt(host[bRR] / host[bBB]) : 0.0;
     return PPT_OK;
 }

@@ -92,9 +92,14 @@ extern "C" int ppt_surface_create(int64_t n_vertices, const double* vertices, in
         *c1 = std::min(std::max((int)std::floor(u1), 0), S.dev.dims[a] - 1);
     };
     std::vector<int64_t> count(cells + 1, 0);
+    std::vector<int32_t> trange((size_t)n_triangles * 6);
     for (int64_t t = 0; t < n_triangles; ++t) {
         int r0[3], r1[3];
-        for (int a = 0; a < 3; ++a) cell_range(t, a, &r0[a], &r1[a]);
+        for (int a = 0; a < 3; ++a) {
+            cell_range(t, a, &r0[a], &r1[a]);
+            trange[6 * t + 2 * a] = r0[a];
+            trange[6 * t + 2 * a + 1] = r1[a];
+        }
         for (int i = r0[0]; i <= r1[0]; ++i)
             for (int j = r0[1]; j <= r1[1]; ++j)
                 for (int k = r0[2]; k <= r1[2]; ++k) ++count[(i * (int64_t)S.dev.dims[1] + j) * S.dev.dims[2] + k + 1];
@@ -115,7 +120,8 @@ extern "C" int ppt_surface_create(int64_t n_vertices, const double* vertices, in
     const size_t b_tri = tri.size() * sizeof(double);
     const size_t b_start = start.size() * sizeof(int32_t);
     const size_t b_list = std::max<size_t>(list.size(), 1) * sizeof(int32_t);
-    S.bytes = b_tri + b_start + b_list;
+    const size_t b_range = trange.size() * sizeof(int32_t);
+    S.bytes = b_tri + b_start + b_list + b_range;
     PPT_CUDA_TRY(cudaGetDevice(&S.device));
     cudaError_t e = cudaMalloc(&S.buf, S.bytes);
     if (e != cudaSuccess) {
@@ -127,6 +133,8 @@ extern "C" int ppt_surface_create(int64_t n_vertices, const double* vertices, in
     if (e == cudaSuccess) e = cudaMemcpy(base + b_tri, start.data(), b_start, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !list.empty())
         e = cudaMemcpy(base + b_tri + b_start, list.data(), list.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(base + b_tri + b_start + b_list, trange.data(), b_range, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         cudaFree(S.buf);
         return cuda_fail(e, "surface upload");
@@ -134,8 +142,35 @@ extern "C" int ppt_surface_create(int64_t n_vertices, const double* vertices, in
     S.dev.tri = reinterpret_cast<const double*>(base);
     S.dev.cell_start = reinterpret_cast<const int32_t*>(base + b_tri);
     S.dev.cell_tri = reinterpret_cast<const int32_t*>(base + b_tri + b_start);
+    S.dev.trange = reinterpret_cast<const int32_t*>(base + b_tri + b_start + b_list);
     S.dev.n_tri = (int32_t)n_triangles;
     *out = new ppt_surface(S);
+    return PPT_OK;
+}
+
+__global__ void axis_rays_kernel(const __grid_constant__ SurfaceDev S, int64_t n, const double* __restrict__ pts,
+                                 double* __restrict__ dist, int32_t* __restrict__ hits) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n * 6) return;
+    const int64_t row = i / 6;
+    const int dir = (int)(i - row * 6);
+    int c;
+    double d;
+    axis_ray_hits(S, v3(pts[3 * row], pts[3 * row + 1], pts[3 * row + 2]), dir, c, d);
+    dist[i] = d;
+    hits[i] = c;
+}
+
+extern "C" int ppt_surface_axis_rays(const ppt_surface* s, int64_t n, const double* points, double* min_dist,
+                                     int32_t* hits, void* stream) {
+    if (!s) return fail(PPT_ERR_ARG, "surface is NULL");
+    if (n < 0) return fail(PPT_ERR_ARG, "n must be >= 0");
+    if (n == 0) return PPT_OK;
+    if (!points || !min_dist || !hits) return fail(PPT_ERR_ARG, "points, min_dist and hits must not be NULL");
+    const int block = 128;
+    axis_rays_kernel<<<grid_for(n * 6, block), block, 0, static_cast<cudaStream_t>(stream)>>>(s->dev, n, points,
+                                                                                              min_dist, hits);
+    PPT_CUDA_TRY(cudaGetLastError());
     return PPT_OK;
 }
 

@@ -15,9 +15,16 @@ zero potential beyond the box; the field is central differences on the
 interior, zero on the outer layer; ``e_field`` is a trilinear ``Field`` on
 the cell centres.  The linear solve is conjugate gradients to
 ``solver_tol`` (the reference: GMRES with an AMG preconditioner to the same
-relative residual).  Conductor cells (electrode geometry from py_electrodes,
-Shortley-Weller boundaries) are not on the GPU path: an electrode assembly
-raises ``NotImplementedError``.
+relative residual).
+
+With an electrode assembly (an ``ElectrodeSurface`` or any object with
+``vertices`` / ``triangles``), the cells are classified as the reference
+does (:241-291) from rays cast along the six axis directions from every cell
+centre (``ppt_surface_axis_rays``): conductor where some ray crosses the
+surface an odd number of times, boundary where a crossing lies within one
+cell size.  Conductor cells hold zero potential; the rows next to them use the
+distances to the surface (Shortley-Weller, :293-443); that operator is not
+symmetric, so the solve is BiCGSTAB (``ppt_poisson_solve_coef``).
 """
 import time
 
@@ -27,6 +34,57 @@ from scipy import constants as _const
 from . import _lib
 
 EPS0 = _const.epsilon_0
+
+INTERIOR, BOUNDARY, CONDUCTOR = 0, 1, 2   # the reference's CellType (poisson_amg.py:86-90)
+
+
+def classify_cells(min_dist, hits, h):
+    """Cell types from the six axis rays of each cell centre
+    (poisson_amg.py:258-281); the cell sizes are compared as float32, as there."""
+    conductor = (hits % 2 != 0).any(axis=1)
+    sizes = np.array([h[0], h[0], h[1], h[1], h[2], h[2]], dtype=np.float32)
+    boundary = (min_dist <= sizes).any(axis=1) & ~conductor
+    kind = np.full(hits.shape[0], INTERIOR, dtype=np.int32)
+    kind[boundary] = BOUNDARY
+    kind[conductor] = CONDUCTOR
+    return kind
+
+
+def operator_coefficients(cells, h, cell_type, dist):
+    """(m, 7) rows of the operator: diagonal and +x, -x, +y, -y, +z, -z
+    couplings, as the reference's assembly loop forms them (poisson_amg.py:
+    322-437): towards a conductor neighbour the spacing is the distance to the
+    surface (at least h / 1000) and the coupling is dropped; a conductor cell's
+    row is the identity."""
+    n = tuple(int(c) for c in cells)
+    kind = np.asarray(cell_type).reshape(n)
+    cond = kind == CONDUCTOR
+    d = np.asarray(dist, dtype=np.float64).reshape(n + (6,))
+    coef = np.zeros(n + (7,))
+    diag = np.zeros(n)
+    for a in range(3):
+        lo = [slice(None)] * 3
+        hi = [slice(None)] * 3
+        lo[a], hi[a] = slice(0, n[a] - 1), slice(1, n[a])
+        lo, hi = tuple(lo), tuple(hi)
+        has_pos = np.zeros(n, dtype=bool)
+        has_pos[lo] = True
+        has_neg = np.zeros(n, dtype=bool)
+        has_neg[hi] = True
+        cond_pos = np.zeros(n, dtype=bool)
+        cond_pos[lo] = cond[hi]
+        cond_neg = np.zeros(n, dtype=bool)
+        cond_neg[hi] = cond[lo]
+        floor = h[a] * 1e-3
+        hp = np.where(cond_pos, np.maximum(d[..., 2 * a], floor), h[a])
+        hn = np.where(cond_neg, np.maximum(d[..., 2 * a + 1], floor), h[a])
+        diag = diag + 2.0 / (hp * hn)
+        coef[..., 1 + 2 * a] = np.where(has_pos & ~cond_pos, -2.0 / (hp * (hp + hn)), 0.0)
+        coef[..., 2 + 2 * a] = np.where(has_neg & ~cond_neg, -2.0 / (hn * (hp + hn)), 0.0)
+    coef[..., 0] = diag
+    coef[cond] = 0.0
+    coef[cond, 0] = 1.0
+    return coef.reshape(-1, 7)
 
 
 class PoissonSolverConfig:
@@ -44,12 +102,11 @@ class PoissonSolverConfig:
 
 
 class SpaceChargeSolver:
-    """GPU counterpart of ``PyAMGPoissonSolver`` for a domain without conductors."""
+    """GPU counterpart of ``PyAMGPoissonSolver`` (conductor cells from an
+    optional electrode assembly)."""
 
     def __init__(self, config, electrode_assembly=None, device=None):
         import torch
-        if electrode_assembly is not None:
-            raise NotImplementedError("conductor cells (electrode geometry) are not on the GPU Poisson path")
         if not torch.cuda.is_available():
             raise RuntimeError("the space-charge solver runs on the GPU (no CPU fallback)")
         self.config = config
@@ -63,10 +120,16 @@ class SpaceChargeSolver:
         for a, (e, c) in enumerate(zip(config.domain_extent, config.mesh_cells)):
             self.mesh.extent[a] = e
             self.mesh.cells[a] = c
-        nbytes = self.lib.ppt_poisson_scratch_bytes(self.mesh)
+        shape = (self.nx, self.ny, self.nz)
+        self.cell_type = None
+        self._coef = None
+        self._conductor = None
+        if electrode_assembly is not None:
+            self._classify(electrode_assembly)
+        nbytes = (self.lib.ppt_poisson_coef_scratch_bytes if self._coef is not None
+                  else self.lib.ppt_poisson_scratch_bytes)(self.mesh)
         if nbytes < 0:
             _lib.check(-1)
-        shape = (self.nx, self.ny, self.nz)
         self._scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         self._rho = torch.empty(shape, dtype=torch.float64, device=self.device)
         self.phi = torch.zeros(shape, dtype=torch.float64, device=self.device)
@@ -75,6 +138,29 @@ class SpaceChargeSolver:
         self.solve_times = []
         self.last_iterations = 0
         self.last_residual = 0.0
+
+    def _classify(self, electrode_assembly):
+        """Cell types and operator rows from the electrode surfaces (the
+        reference's one-time setup, poisson_amg.py:241-443)."""
+        import torch
+        from .electrodes import ElectrodeSurface
+        surf = ElectrodeSurface.from_assembly(electrode_assembly)
+        gx, gy, gz = self.cell_centres()
+        xx, yy, zz = np.meshgrid(gx, gy, gz, indexing="ij")
+        nodes = torch.from_numpy(np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()])).to(self.device)
+        dist = torch.empty((self.n_dofs, 6), dtype=torch.float64, device=self.device)
+        hits = torch.empty((self.n_dofs, 6), dtype=torch.int32, device=self.device)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.ppt_surface_axis_rays(surf.handle(self.device), self.n_dofs, nodes.data_ptr(),
+                                                      dist.data_ptr(), hits.data_ptr(), _lib.stream_handle()))
+        self.boundary_distances = dist.cpu().numpy()
+        self.hit_counts = hits.cpu().numpy()
+        h = (self.hx, self.hy, self.hz)
+        self.cell_type = classify_cells(self.boundary_distances, self.hit_counts, h)
+        coef = operator_coefficients((self.nx, self.ny, self.nz), h, self.cell_type, self.boundary_distances)
+        self._coef = torch.from_numpy(coef).to(self.device)
+        self._conductor = torch.from_numpy(self.cell_type == CONDUCTOR).to(self.device).reshape(
+            self.nx, self.ny, self.nz)
 
     def cell_centres(self):
         """The solver's cell-centre coordinates per axis (poisson_amg.py:229-231)."""
@@ -93,9 +179,18 @@ class SpaceChargeSolver:
         self._rho.div_(EPS0)                 # rhs = rho / eps0 (poisson_amg.py:917)
         self.phi.zero_()                     # the reference starts GMRES from zero
         iters, res = _lib.c_int64(), _lib.c_double()
-        _lib.check(self.lib.ppt_poisson_solve(self.mesh, self._rho.data_ptr(), self.phi.data_ptr(),
-                                              self._scratch.data_ptr(), self.config.solver_tol,
-                                              self.config.max_iterations, iters, res, st))
+        if self._coef is None:
+            _lib.check(self.lib.ppt_poisson_solve(self.mesh, self._rho.data_ptr(), self.phi.data_ptr(),
+                                                  self._scratch.data_ptr(), self.config.solver_tol,
+                                                  self.config.max_iterations, iters, res, st))
+        else:
+            # conductor cells: zero potential, their charge dropped (:919-921, :727-729)
+            self._rho.masked_fill_(self._conductor, 0.0)
+            _lib.check(self.lib.ppt_poisson_solve_coef(self.mesh, self._coef.data_ptr(), self._rho.data_ptr(),
+                                                       self.phi.data_ptr(), self._scratch.data_ptr(),
+                                                       self.config.solver_tol, self.config.max_iterations,
+                                                       iters, res, st))
+            self.phi.masked_fill_(self._conductor, 0.0)
         self.last_iterations, self.last_residual = iters.value, res.value
         _lib.check(self.lib.ppt_field_from_potential(self.mesh, self.phi.data_ptr(), self.e[0].data_ptr(),
                                                      self.e[1].data_ptr(), self.e[2].data_ptr(), st))

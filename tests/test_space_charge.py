@@ -1,11 +1,13 @@
 """Space-charge solve: deposition, Poisson solve and E = -grad phi
-(PyAMGPoissonSolver, src/PyPATools/poisson_amg.py) for a domain without
+(PyAMGPoissonSolver, src/PyPATools/poisson_amg.py), with and without
 conductor cells.
 
-The oracle's operator and field step are pinned bit for bit to the
-reference's own matrix assembly and field function (tests/golden/
-poisson_golden.npz, made by make_golden_poisson.py).  The GPU solve is held to
-the exact solution of that operator (sparse direct solve) at 1e-8 relative
+The oracle's operator, cell classification, Shortley-Weller rows and field
+step are pinned bit for bit to the reference's own code (tests/golden/
+poisson_golden.npz, made by make_golden_poisson.py; the classification runs
+on ray results served to it, since its electrode package is not installed).
+The GPU ray casting matches the oracle's bit for bit; the GPU solves are held
+to the exact solution of the operator (sparse direct solve) at 1e-8 relative
 when solved to a 1e-12 residual; the field step to the reference bit for bit."""
 import ctypes
 
@@ -57,6 +59,48 @@ def test_poisson_argument_checks_without_gpu():
     bad = _mesh((0.1, -1.0, 0.1), (4, 4, 4))
     assert lib.ppt_field_from_potential(bad, ctypes.c_void_p(16), None, None, None, None) == -1
     assert b"positive" in lib.ppt_last_error()
+
+
+def _cond():
+    cells = tuple(int(c) for c in G["cond/cells"])
+    h = [G["cond/extent"][a] / cells[a] for a in range(3)]
+    return G["cond/extent"], cells, h
+
+
+def test_oracle_conductor_classification_and_rows_match_reference():
+    extent, cells, h = _cond()
+    kind = sco.classify_cells(G["cond/dist"], G["cond/hits"], h)
+    np.testing.assert_array_equal(kind, G["cond/cell_type"])
+    a, keep = sco.assemble_reduced(extent, cells, kind, G["cond/dist"])
+    np.testing.assert_array_equal(keep, G["cond/keep"])
+    ref = sp.csr_matrix((G["cond/A_val"], (G["cond/A_row"], G["cond/A_col"])), shape=a.shape)
+    np.testing.assert_array_equal(a.toarray(), ref.toarray())
+
+
+def test_product_rows_match_oracle():
+    # the solver's (m, 7) coefficient rows are the reference's reduced matrix
+    # on the non-conductor cells and the identity on the conductor ones
+    from pypatools_b200.space_charge import classify_cells, operator_coefficients
+    extent, cells, h = _cond()
+    kind = classify_cells(G["cond/dist"], G["cond/hits"], h)
+    np.testing.assert_array_equal(kind, G["cond/cell_type"])
+    coef = operator_coefficients(cells, h, kind, G["cond/dist"])
+    m = coef.shape[0]
+    strides = (cells[1] * cells[2], cells[2], 1)
+    rows, cols, vals = [], [], []
+    for c in range(m):
+        rows.append(c); cols.append(c); vals.append(coef[c, 0])
+        for a in range(3):
+            for k, sgn in ((1 + 2 * a, 1), (2 + 2 * a, -1)):
+                if coef[c, k] != 0.0:
+                    rows.append(c); cols.append(c + sgn * strides[a]); vals.append(coef[c, k])
+    full = sp.csr_matrix((vals, (rows, cols)), shape=(m, m)).toarray()
+    keep = G["cond/keep"]
+    ref = sp.csr_matrix((G["cond/A_val"], (G["cond/A_row"], G["cond/A_col"])), shape=(keep.size, keep.size))
+    np.testing.assert_array_equal(full[np.ix_(keep, keep)], ref.toarray())
+    cond = np.setdiff1d(np.arange(m), keep)
+    np.testing.assert_array_equal(full[cond], np.eye(m)[cond])
+    assert not full[np.ix_(keep, cond)].any()
 
 
 @pytest.mark.gpu
@@ -129,3 +173,60 @@ def test_gpu_space_charge_solve_vs_oracle(cuda):
     assert not np.any(phi0) and solver.last_iterations == 0
     with pytest.raises(NotImplementedError):
         SpaceChargeSolver(PoissonSolverConfig(extent, cells), electrode_assembly=object())
+
+
+def _electrode_case():
+    from pypatools_b200.electrodes import ElectrodeSurface
+    # a beam pipe (radius 15 mm) with an aperture plate (hole 6 mm) at z = 0
+    return ElectrodeSurface.tube(0.015, -0.05, 0.05, n_phi=40, n_z=10) + \
+        ElectrodeSurface.aperture_plate(0.0, 0.006, 0.015, n_phi=40, n_r=3)
+
+
+@pytest.mark.gpu
+def test_gpu_axis_rays_match_oracle_bitwise(cuda):
+    torch = cuda
+    s = _electrode_case()
+    rng = np.random.default_rng(12)
+    pts = np.column_stack([rng.uniform(-0.02, 0.02, 3000), rng.uniform(-0.02, 0.02, 3000),
+                           rng.uniform(-0.06, 0.06, 3000)])
+    pts = np.concatenate([pts, [[0.0, 0.0, 0.0], [0.015, 0.0, 0.01], [0.0, 0.0, 0.07]]])
+    d_p = torch.from_numpy(pts).cuda()
+    dist = torch.empty((pts.shape[0], 6), dtype=torch.float64, device="cuda")
+    hits = torch.empty((pts.shape[0], 6), dtype=torch.int32, device="cuda")
+    _lib.check(_lib.load().ppt_surface_axis_rays(s.handle("cuda"), pts.shape[0], d_p.data_ptr(), dist.data_ptr(),
+                                                 hits.data_ptr(), _lib.stream_handle()))
+    ref_d, ref_h = sco.axis_ray_hits(pts, s.vertices, s.triangles)
+    np.testing.assert_array_equal(hits.cpu().numpy(), ref_h)
+    np.testing.assert_array_equal(dist.cpu().numpy(), ref_d)
+    assert (ref_h % 2 == 1).any() and (ref_h == 0).any()
+
+
+@pytest.mark.gpu
+def test_gpu_space_charge_with_conductors_vs_oracle(cuda):
+    from pypatools_b200.space_charge import PoissonSolverConfig, SpaceChargeSolver, CONDUCTOR
+    s = _electrode_case()
+    extent, cells = (0.04, 0.04, 0.1), (16, 16, 40)
+    rng = np.random.default_rng(13)
+    n = 20000
+    p = np.column_stack([rng.normal(0, 2e-3, n), rng.normal(0, 2e-3, n), rng.normal(0.02, 8e-3, n)])
+    q = np.full(n, 1.602176634e-19 * 1e5)
+    solver = SpaceChargeSolver(PoissonSolverConfig(extent, cells, solver_tol=1e-12, max_iterations=20000),
+                               electrode_assembly=s)
+    kind = solver.cell_type
+    assert (kind == CONDUCTOR).sum() > 100 and (kind == 1).sum() > 100
+    # the cell types come from the same rays as the oracle's
+    gx, gy, gz = solver.cell_centres()
+    xx, yy, zz = np.meshgrid(gx, gy, gz, indexing="ij")
+    ref_d, ref_h = sco.axis_ray_hits(np.column_stack([xx.ravel(), yy.ravel(), zz.ravel()]), s.vertices,
+                                     s.triangles)
+    h = (solver.hx, solver.hy, solver.hz)
+    np.testing.assert_array_equal(kind, sco.classify_cells(ref_d, ref_h, h))
+    phi, _ = solver.solve(p, q)
+    assert solver.last_residual <= 1e-12
+    a, keep = sco.assemble_reduced(extent, cells, kind, ref_d)
+    rho = sco.bin_particles_cic(p, q, extent, cells).reshape(-1)
+    x = np.zeros(kind.size)
+    x[keep] = sco.spsolve(a.tocsc(), (rho / sco.EPS0)[keep])
+    x = x.reshape(cells)
+    np.testing.assert_allclose(phi, x, rtol=0, atol=1e-8 * np.abs(x).max())
+    assert not phi.reshape(-1)[kind == CONDUCTOR].any()
