@@ -12,7 +12,9 @@ inside the float64 track kernel, step by step.
 ``PusherGPU`` accepts an ``ElectrodeSurface`` or any object with ``vertices``
 ((V, 3) float) and ``triangles`` ((T, 3) int) arrays describing the electrode
 surfaces.  The builders below make the simple shapes of beam-line tests: an
-aperture plate (an annulus in a z plane) and a tube (a cylinder along z).
+aperture plate (an annulus in a z plane), a tube (a cylinder along z), and a
+closed annular cylinder (a thick pipe or plate, for the space-charge solver's
+conductor cells, which need closed surfaces).
 """
 import ctypes
 import math
@@ -122,6 +124,16 @@ class ElectrodeSurface:
                 c, d = a + n_phi, b + n_phi
                 tris += [[a, b, d], [a, d, c]]
         return cls(verts, np.array(tris))
+
+    @classmethod
+    def annular_cylinder(cls, r_in, r_out, z0, z1, n_phi=64, n_z=16, n_r=2):
+        """A closed solid: the ring r_in <= r <= r_out, z0 <= z <= z1 (a thick
+        beam pipe, or a thick aperture plate when z1 - z0 is small).  Its
+        surface is closed, so rays from inside the solid cross it an odd number
+        of times (the conductor test of the space-charge solver); the other
+        builders make open sheets, enough for stopping particles."""
+        return (cls.tube(r_out, z0, z1, n_phi, n_z) + cls.tube(r_in, z0, z1, n_phi, n_z) +
+                cls.aperture_plate(z0, r_in, r_out, n_phi, n_r) + cls.aperture_plate(z1, r_in, r_out, n_phi, n_r))
 
     @classmethod
     def tube(cls, radius, z0, z1, n_phi=64, n_z=16):

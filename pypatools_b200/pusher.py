@@ -302,6 +302,84 @@ class DeviceTracker:
         return {"map_hits": int(c[0]), "particle_steps": int(c[1])}
 
 
+class HostStager:
+    """Device -> numpy copies through a ring of pinned buffers.
+
+    Each piece (``chunk`` bytes at most) goes device -> pinned buffer on a copy
+    stream (PCIe at full speed, ~50 GB/s on B200 hosts), then a worker thread
+    copies it into the destination numpy array (numpy releases the GIL for
+    the copy, which also maps the fresh array's pages); the ring keeps
+    ``slots`` pieces in flight.  Pinning the destination instead costs about a
+    second per 1.5 GB whenever the caller still holds earlier results, and a
+    device copy into pageable memory runs at ~2 GB/s.  Measured on the 1e7
+    proton x 41-record job (19.7 GB of histories): 0.70-0.73 s per call with
+    24 slots of 32 MB, kept or dropped results alike (6 x 128 MB: 1.05 s;
+    pinning the whole histories: 0.70 s while torch's pinned cache can reuse a
+    dropped result, 14 s when the caller keeps them; touching the fresh
+    pages from a second thread group first: 0.79 s)."""
+
+    _by_device = {}
+
+    def __init__(self, device, chunk=32 << 20, slots=24):
+        import threading
+        from concurrent.futures import ThreadPoolExecutor
+        torch = _torch()
+        self.torch = torch
+        self.device = device
+        self.chunk = int(chunk)
+        self.buffers = [torch.empty(self.chunk, dtype=torch.uint8, pin_memory=True) for _ in range(slots)]
+        self.views = [b.numpy() for b in self.buffers]
+        self.events = [torch.cuda.Event() for _ in range(slots)]
+        self.pending = [None] * slots
+        self.next = 0
+        self.stream = torch.cuda.Stream(device=device)
+        self.pool = ThreadPoolExecutor(max_workers=slots)
+        self.lock = threading.Lock()
+
+    @classmethod
+    def for_device(cls, device):
+        import torch
+        key = torch.device(device).index if torch.device(device).index is not None else torch.cuda.current_device()
+        st = cls._by_device.get(key)
+        if st is None:
+            st = cls._by_device[key] = cls(torch.device("cuda", key))
+        return st
+
+    def copy(self, src, dst, after=None):
+        """Queue the copy of the contiguous device tensor ``src`` into the
+        contiguous numpy array ``dst`` (same bytes), after event ``after``."""
+        with self.lock:
+            self._copy(src, dst, after)
+
+    def _copy(self, src, dst, after):
+        torch = self.torch
+        sb = src.reshape(-1).view(torch.uint8)
+        db = dst.reshape(-1).view(np.uint8)
+        if after is not None:
+            self.stream.wait_event(after)
+        for a in range(0, db.size, self.chunk):
+            b = min(a + self.chunk, db.size)
+            k = self.next
+            self.next = (k + 1) % len(self.buffers)
+            if self.pending[k] is not None:
+                self.pending[k].result()          # the slot's previous piece is in its numpy array
+            with torch.cuda.stream(self.stream):
+                self.buffers[k][:b - a].copy_(sb[a:b], non_blocking=True)
+                self.events[k].record(self.stream)
+            self.pending[k] = self.pool.submit(self._land, k, db, a, b)
+
+    def _land(self, k, db, a, b):
+        self.events[k].synchronize()
+        np.copyto(db[a:b], self.views[k][:b - a])
+
+    def finish(self):
+        with self.lock:
+            for k, f in enumerate(self.pending):
+                if f is not None:
+                    f.result()
+                    self.pending[k] = None
+
+
 class PusherGPU:
     """Batch and single-particle tracking on the GPU with the reference's API."""
 
@@ -445,12 +523,13 @@ class PusherGPU:
         to_host = self.snapshot == "host"
         with torch.cuda.device(df.device):
             if to_host:
-                # Snapshot rows stream to pinned host memory on a copy stream
-                # while later launches run; torch's pinned-block cache makes
-                # repeated calls of one size cheap.
-                h_r = torch.empty((n_rec, m, 3), dtype=torch.float64, pin_memory=True)
-                h_v = torch.empty((n_rec, m, 3), dtype=torch.float64, pin_memory=True)
-                copy_stream = torch.cuda.Stream(device=df.device)
+                # Snapshot rows stream to the numpy results while later
+                # launches run: finished rows go through a small ring of
+                # pinned buffers (HostStager) instead of pinning the whole
+                # histories, which costs seconds per call for large bunches.
+                h_r = np.empty((n_rec, m, 3))
+                h_v = np.empty((n_rec, m, 3))
+                stager = HostStager.for_device(df.device)
                 compute = torch.cuda.current_stream()
                 copied = 0
 
@@ -460,10 +539,8 @@ class PusherGPU:
                         return
                     ev = torch.cuda.Event()
                     ev.record(compute)
-                    copy_stream.wait_event(ev)
-                    with torch.cuda.stream(copy_stream):
-                        h_r[copied:upto].copy_(tr.r_hist[copied:upto], non_blocking=True)
-                        h_v[copied:upto].copy_(tr.v_hist[copied:upto], non_blocking=True)
+                    stager.copy(tr.r_hist[copied:upto], h_r[copied:upto], ev)
+                    stager.copy(tr.v_hist[copied:upto], h_v[copied:upto], ev)
                     copied = upto
             tr.load(self._upload(r0, df.device), self._upload(v0, df.device))
 
@@ -478,7 +555,7 @@ class PusherGPU:
             tr.run(nsteps, chunk, sort_every=sort_every, after_launch=after_launch)
             if to_host:
                 drain(n_rec)
-                copy_stream.synchronize()
+                stager.finish()
             status = tr.device_status()
         if status & _lib.STATUS_NONFINITE:
             warnings.warn("non-finite particle state encountered during tracking", RuntimeWarning)
@@ -490,7 +567,7 @@ class PusherGPU:
         active = np.ones(m, dtype=bool) if tr.active is None else tr.active.cpu().numpy().astype(bool)
         if not to_host:
             return tr.r_hist, tr.v_hist, active
-        return h_r.numpy(), h_v.numpy(), active
+        return h_r, h_v, active
 
     # -- single-particle API -------------------------------------------------
     def push(self, r, v, efield, bfield, dt):

@@ -177,9 +177,10 @@ def test_gpu_space_charge_solve_vs_oracle(cuda):
 
 def _electrode_case():
     from pypatools_b200.electrodes import ElectrodeSurface
-    # a beam pipe (radius 15 mm) with an aperture plate (hole 6 mm) at z = 0
-    return ElectrodeSurface.tube(0.015, -0.05, 0.05, n_phi=40, n_z=10) + \
-        ElectrodeSurface.aperture_plate(0.0, 0.006, 0.015, n_phi=40, n_r=3)
+    # closed solids: a thick beam pipe (wall 12-16 mm) and a 4 mm thick
+    # aperture plate (hole 5 mm) at z = 0
+    return ElectrodeSurface.annular_cylinder(0.012, 0.016, -0.05, 0.05, n_phi=40, n_z=10) + \
+        ElectrodeSurface.annular_cylinder(0.005, 0.012, -0.002, 0.002, n_phi=40, n_z=1)
 
 
 @pytest.mark.gpu
@@ -214,6 +215,10 @@ def test_gpu_space_charge_with_conductors_vs_oracle(cuda):
                                electrode_assembly=s)
     kind = solver.cell_type
     assert (kind == CONDUCTOR).sum() > 100 and (kind == 1).sum() > 100
+    # the pipe's inside is vacuum, its wall and the plate are conductor
+    assert kind.reshape(cells)[8, 8, 30] == 0 and kind.reshape(cells)[2, 8, 30] == CONDUCTOR
+    assert kind.reshape(cells)[1, 8, 30] == 1           # just outside the wall
+    assert kind.reshape(cells)[3, 8, 20] == CONDUCTOR
     # the cell types come from the same rays as the oracle's
     gx, gy, gz = solver.cell_centres()
     xx, yy, zz = np.meshgrid(gx, gy, gz, indexing="ij")
