@@ -87,11 +87,18 @@ extern "C" int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_trac
         }
         return launch_track_f64(P, st->algorithm, rf, a->surface != nullptr, s);
     }
-    if (a->surface)
-        return fail(PPT_ERR_UNSUPPORTED, "electrode surfaces run in the float64 form only");
+    if (a->surface && st->algorithm != PPT_ALG_BORIS)
+        return fail(PPT_ERR_UNSUPPORTED, "electrode surfaces run in the float64 form and the mixed form's boris");
+    if (a->surface && !a->active) return fail(PPT_ERR_ARG, "a surface needs the active array");
     TrackMixDev P;
     std::memset(&P, 0, sizeof(P));
     rc = make_track_mixed(F, st, a, n_rec, &P);
     if (rc) return rc;
+    if (a->surface) {
+        CollDev C;
+        C.surf = a->surface->dev;
+        C.active = a->active;
+        return launch_track_mixed_coll(P, C, rf, s);
+    }
     return launch_track_mixed(P, st->algorithm, rf, s);
 }

@@ -581,10 +581,26 @@ __device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t re
     }
 }
 
-template <int ALG, bool RF, int L>
-__device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, int64_t s, MixCtx& c) {
+// float64 position of (cell + offset) on the tracking grid (the snapshot rows' formula)
+__device__ __forceinline__ V3 mixed_position(const TrackMixDev& P, const float cf[3], const float f[3]) {
+    return v3(P.G.lo[0] + ((double)cf[0] + (double)f[0]) * P.G.d[0],
+              P.G.lo[1] + ((double)cf[1] + (double)f[1]) * P.G.d[1],
+              P.G.lo[2] + ((double)cf[2] + (double)f[2]) * P.G.d[2]);
+}
+
+// COLL (Boris only): each step's segment, from the float64 positions before
+// and after it, is tested against the electrode surface after the step's
+// snapshot, and a particle that hits stops there (pusher.py:966-990).
+template <int ALG, bool RF, int L, bool COLL = false>
+__device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, int64_t s, MixCtx& c,
+                                                         const CollDev* C = nullptr) {
     {
         const int64_t n = P.n;
+        if constexpr (COLL) {
+            if (!C->active[P.order ? P.order[s] : s]) return 0;   // stopped in an earlier call
+        }
+        bool stopped = false;
+        unsigned steps_done = (unsigned)P.nsteps;
         int cell[3];
         float f[3], vh[3], vl[3];
 #pragma unroll
@@ -626,6 +642,34 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 const int64_t to_rec = (int64_t)until + 1;
                 const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
                 const int64_t g0 = P.step0 + k;
+                if constexpr (COLL) {
+                    // one step at a time, each segment tested (no field-free runs)
+                    int i = 0;
+                    while (i < seg) {
+                        const V3 r0 = mixed_position(P, cf, f);
+                        family_step<ALG, RF, L>(c, cf, f, vh, vl, d, g0 + i);
+                        ++i;
+                        if (segment_hits_surface(C->surf, r0, mixed_position(P, cf, f))) {
+                            stopped = true;
+                            break;
+                        }
+                    }
+                    k += i;
+                    // the reference records the step's position before its collision test
+                    if ((int64_t)i == to_rec) {
+                        const int64_t rec = (P.step0 + k) / P.rec_every;
+                        const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
+                        if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
+                        until = rec_every - 1;
+                    } else {
+                        until -= i;
+                    }
+                    if (stopped) {
+                        steps_done = (unsigned)k;
+                        break;
+                    }
+                    continue;
+                }
                 for (int i = 0; i < seg;) {
                     if (quiet > 0) {
                         const int m = quiet < seg - i ? quiet : seg - i;
@@ -662,7 +706,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 }
             }
         }
-        if (P.flags & PPT_TRACK_FINAL) {
+        if ((P.flags & PPT_TRACK_FINAL) && !stopped) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
                 int cn[3];
@@ -692,8 +736,11 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             const int lim = 1 << 24;
             if (abs(cell[0]) >= lim || abs(cell[1]) >= lim || abs(cell[2]) >= lim) atomicOr(P.status, PPT_STATUS_RANGE);
         }
+        if constexpr (COLL) {
+            if (stopped) C->active[P.order ? P.order[s] : s] = 0;
+        }
+        return steps_done;
     }
-    return (unsigned)P.nsteps;
 }
 
 template <int ALG, bool RF, int L>
@@ -710,6 +757,25 @@ __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant_
         }
     }
     if (s < P.n) steps_done = track_mixed_particle<ALG, RF, L>(P, s, c);
+    if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
+}
+
+// The same with the electrode segment test (Boris).
+template <bool RF, int L>
+__global__ void __launch_bounds__(128) track_mixed_coll_kernel(const __grid_constant__ TrackMixDev P,
+                                                               const __grid_constant__ CollDev C) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned steps_done = 0;
+    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, nullptr, 0};
+    if constexpr (RF) {
+        extern __shared__ float2 rf_tab[];
+        if (P.rf_tab_n > 0) {
+            build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
+            c.tab = rf_tab;
+            c.tab0 = P.step0;
+        }
+    }
+    if (s < P.n) steps_done = track_mixed_particle<PPT_ALG_BORIS, RF, L, true>(P, s, c, &C);
     if (P.counters) block_add_counters(P.counters, c.hits, steps_done);
 }
 
@@ -819,6 +885,30 @@ int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, int layout, bool rf, 
 
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s) {
     return launch_mixed(&P, nullptr, algorithm, P.map.layout, rf, 0, s, "track_mixed_kernel launch");
+}
+
+template <int L>
+static cudaError_t launch_coll_layout(const TrackMixDev& P, const CollDev& C, bool rf, cudaStream_t s) {
+    constexpr bool kE = layout_has_e(L);
+    const int block = pick_block(P.n);
+    const int g = grid_for(P.n, block);
+    if (rf && kE) track_mixed_coll_kernel<kE, L><<<g, block, (size_t)P.rf_tab_n * sizeof(float2), s>>>(P, C);
+    else track_mixed_coll_kernel<false, L><<<g, block, 0, s>>>(P, C);
+    return cudaGetLastError();
+}
+
+int launch_track_mixed_coll(const TrackMixDev& P, const CollDev& C, bool rf, cudaStream_t s) {
+    cudaError_t e;
+    switch (P.map.layout) {
+        case kLayFull: e = launch_coll_layout<kLayFull>(P, C, rf, s); break;
+        case kLayE: e = launch_coll_layout<kLayE>(P, C, rf, s); break;
+        case kLayB: e = launch_coll_layout<kLayB>(P, C, rf, s); break;
+        case kLayExEyBz: e = launch_coll_layout<kLayExEyBz>(P, C, rf, s); break;
+        case kLayEzBz: e = launch_coll_layout<kLayEzBz>(P, C, rf, s); break;
+        default: e = launch_coll_layout<kLayBz>(P, C, rf, s); break;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "track_mixed_coll_kernel launch");
+    return PPT_OK;
 }
 
 // host-side construction of the mixed kernel parameters

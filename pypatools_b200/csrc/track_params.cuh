@@ -68,6 +68,13 @@ struct TrackMixDev {
     int32_t k_elems;    // map elements per z cell: the record width, 0 when the map does not vary along z
 };
 
+// The electrode surface of a mixed-form Boris track (a second kernel
+// parameter, so the parameter block of the kernels without one stays as it is).
+struct CollDev {
+    SurfaceDev surf;
+    uint8_t* active;    // row order; 0 = stopped by the surface
+};
+
 // One (form, algorithm, RF) class of serving jobs: a block-level work queue
 // over items = (job, 128-particle block) pairs.  The job tables, the per-job
 // step counters and done flags live in device memory, so a tick needs no
@@ -93,6 +100,7 @@ int launch_track_f64(const TrackDev& P, int algorithm, bool rf, bool surface, cu
 int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_args* a, int64_t n_rec,
                      TrackMixDev* P);
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s);
+int launch_track_mixed_coll(const TrackMixDev& P, const CollDev& C, bool rf, cudaStream_t s);
 int launch_f64_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s);
 int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, int layout, bool rf, int grid, cudaStream_t s);
 

@@ -121,8 +121,9 @@ class DeviceTracker:
         self.surface = None
         self.active = None
         if surface is not None:
-            if precision != "fp64":
-                raise NotImplementedError("electrode surfaces run in the float64 form; use precision='fp64'")
+            if precision != "fp64" and algorithm != "boris":
+                raise NotImplementedError("electrode surfaces run in the float64 form and in the mixed form's "
+                                          "boris; use precision='fp64'")
             self.surface = surface.handle(dev)
             self.active = torch.ones(n, dtype=torch.uint8, device=dev)
         if record:
@@ -402,8 +403,9 @@ class PusherGPU:
         if electrode_assembly is not None:
             from .electrodes import ElectrodeSurface
             self.surface = ElectrodeSurface.from_assembly(electrode_assembly)
-            if precision != "fp64":
-                raise NotImplementedError("electrode surfaces run in the float64 form; use precision='fp64'")
+            if precision != "fp64" and algorithm != "boris":
+                raise NotImplementedError("electrode surfaces run in the float64 form and in the mixed form's "
+                                          "boris; use precision='fp64'")
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         if snapshot not in ("host", "device"):
