@@ -27,6 +27,7 @@ prints are left out.
 import gc
 import os
 import re
+import warnings
 
 import numpy as np
 
@@ -40,9 +41,18 @@ UNIT_CONVERSIONS = {
 
 
 def _numbers(lines):
-    """All whitespace-separated numbers of ``lines`` as one float64 array."""
-    text = " ".join(line for line in lines if line.strip())
-    return np.array(text.split(), dtype=np.float64) if text.strip() else np.zeros(0)
+    """All whitespace-separated numbers of ``lines`` as one float64 array
+    (parsed in C, without a Python object per number: a 256^3 map has 1e8)."""
+    text = " ".join(lines)
+    if not text.strip():
+        return np.zeros(0)
+    with warnings.catch_warnings():
+        # numpy warns (and stops) at text it cannot read: make that an error
+        warnings.simplefilter("error")
+        try:
+            return np.fromstring(text, dtype=np.float64, sep=" ")
+        except (DeprecationWarning, ValueError) as exc:
+            raise ValueError(f"could not convert the map's values to numbers: {exc}")
 
 
 def _unit_kind(unit):
