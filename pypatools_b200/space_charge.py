@@ -171,8 +171,13 @@ class SpaceChargeSolver:
     def solve_device(self, particles, charges, stream=None):
         """Deposit, solve and differentiate on the device.  particles: (M,3)
         float64 CUDA tensor, charges: (M,) float64 CUDA tensor.  Leaves phi in
-        ``self.phi`` and (Ex, Ey, Ez) in ``self.e``; returns them."""
-        st = _lib.stream_handle(stream)
+        ``self.phi`` and (Ex, Ey, Ez) in ``self.e``; returns them.  Everything
+        runs on ``stream`` (default: the current stream)."""
+        import torch
+        if stream is not None:
+            with torch.cuda.stream(stream):
+                return self.solve_device(particles, charges)
+        st = _lib.stream_handle()
         m = int(particles.shape[0])
         _lib.check(self.lib.ppt_deposit_cic(m, particles.data_ptr() if m else None,
                                             charges.data_ptr() if m else None, self.mesh, self._rho.data_ptr(), st))
