@@ -88,11 +88,24 @@ def _interp_grid_values(interp):
 _zero_cache = {}
 
 
+def _is_tensor(a):
+    return type(a).__module__.startswith("torch") and hasattr(a, "data_ptr")
+
+
 def _all_zero(values):
     """True when a node array is identically zero.  Remembered per array
     object (validated through a weak reference, so an array allocated later
-    at a freed one's address is scanned afresh); node arrays are treated as
-    immutable once a field uses them."""
+    at a freed one's address is scanned afresh); numpy node arrays are
+    treated as immutable once a field uses them, torch tensors are rescanned
+    after an in-place change (their version counter)."""
+    if _is_tensor(values):
+        key = (id(values), values._version)
+        hit = _zero_cache.get(key)
+        if hit is not None and hit[0]() is values:
+            return hit[1]
+        result = not bool(values.any())
+        _zero_cache[key] = (weakref.ref(values), result)
+        return result
     a = np.asarray(values)
     key = id(a)
     hit = _zero_cache.get(key)
@@ -253,16 +266,21 @@ class DeviceFields:
         scales = (_lib.c_double * 6)()
         base = 0 if kind == "e" else 3
         # components outside the mask are identically zero: nothing to add
-        present = [(ci, np.asarray(term.comps[c])) for ci, c in enumerate("xyz")
-                   if term.comps.get(c) is not None and mask & (1 << (base + ci))]
+        present = [(ci, term.comps[c] if _is_tensor(term.comps[c]) else np.asarray(term.comps[c]))
+                   for ci, c in enumerate("xyz") if term.comps.get(c) is not None and mask & (1 << (base + ci))]
         if not present:
             return
         # float32 node values stay float32 (exact); anything else goes as float64
-        all_f32 = all(a.dtype == np.float32 for _, a in present)
+        all_f32 = all(str(a.dtype) in ("float32", "torch.float32") for _, a in present)
         np_dtype, src_dtype = (np.float32, _lib.DTYPE_F32) if all_f32 else (np.float64, _lib.DTYPE_F64)
+        t_dtype = torch.float32 if all_f32 else torch.float64
         keep = []
         for ci, a in present:
-            tdev = torch.from_numpy(np.ascontiguousarray(a, dtype=np_dtype)).to(self.device)
+            if _is_tensor(a):
+                # device node values (a space-charge field) go straight into the map
+                tdev = a.to(device=self.device, dtype=t_dtype).contiguous()
+            else:
+                tdev = torch.from_numpy(np.ascontiguousarray(a, dtype=np_dtype)).to(self.device)
             keep.append(tdev)
             slot = ci + (0 if kind == "e" else 3)
             ptrs[slot] = tdev.data_ptr()
@@ -301,8 +319,12 @@ class FieldCache:
     @staticmethod
     def _fingerprint(field):
         ft = decompose(field)
+
+        def ident(a):   # a torch tensor changed in place is a new field
+            return (id(a), a._version) if _is_tensor(a) else id(a)
         return (tuple(ft.const.tolist()),
-                tuple((id(t.comps.get("x")), id(t.comps.get("y")), id(t.comps.get("z")), t.scale) for t in ft.terms))
+                tuple((ident(t.comps.get("x")), ident(t.comps.get("y")), ident(t.comps.get("z")), t.scale)
+                      for t in ft.terms))
 
     def get(self, efield, bfield, precision, device=None):
         key = (id(efield), id(bfield), precision, str(device),

@@ -263,11 +263,16 @@ class CudaInterpolator:
         self.bounds_error = bounds_error
         self.fill_value = float(fill_value)
         self._grid = tuple(np.ascontiguousarray(p, dtype=np.float64) for p in points)
-        vals = np.asarray(values)
-        self._values = np.ascontiguousarray(vals, dtype=np.float32 if vals.dtype == np.float32 else np.float64)
+        if type(values).__module__.startswith("torch"):
+            # device node values (e.g. a space-charge field): kept on the device
+            import torch
+            self._values = values.to(torch.float32 if values.dtype == torch.float32 else torch.float64).contiguous()
+        else:
+            vals = np.asarray(values)
+            self._values = np.ascontiguousarray(vals, dtype=np.float32 if vals.dtype == np.float32 else np.float64)
         self._bounds = tuple((float(g[0]), float(g[-1])) for g in self._grid)
         expected = tuple(len(g) for g in self._grid)
-        if self._values.shape != expected:
+        if tuple(self._values.shape) != expected:
             raise ValueError(f"Values shape {self._values.shape} does not match grid shape {expected}")
 
     def __call__(self, xi, method=None):

@@ -201,6 +201,20 @@ class SpaceChargeSolver:
                                                      self.e[1].data_ptr(), self.e[2].data_ptr(), st))
         return self.phi, self.e
 
+    def solve_field_device(self, particles, charges, stream=None):
+        """(phi tensor, E Field) with the field's node values left on the
+        device: a tracker built from it copies them into its map device to
+        device, so a space-charge step feeds the next push without a host
+        round trip.  particles / charges: CUDA tensors."""
+        from .field import Field
+        phi, e = self.solve_device(particles, charges, stream)
+        gx, gy, gz = self.cell_centres()
+        field = Field.from_arrays({"x": gx, "y": gy, "z": gz}, {"x": e[0].clone(), "y": e[1].clone(), "z": e[2].clone()},
+                                  label=f"Space-charge E-field (turn {self.turn_count})", dim=3, scaling=1.0,
+                                  units="m", method="linear", interpolator_backend="auto")
+        self.turn_count += 1
+        return phi.clone(), field
+
     def solve(self, particles, charges):
         """(phi_3d (nx, ny, nz) numpy [V], E_field Field [V/m]) as the
         reference's ``solve`` returns (poisson_amg.py:616-797)."""

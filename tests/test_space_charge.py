@@ -235,3 +235,44 @@ def test_gpu_space_charge_with_conductors_vs_oracle(cuda):
     x = x.reshape(cells)
     np.testing.assert_allclose(phi, x, rtol=0, atol=1e-8 * np.abs(x).max())
     assert not phi.reshape(-1)[kind == CONDUCTOR].any()
+
+
+@pytest.mark.gpu
+def test_gpu_space_charge_field_feeds_the_pusher_on_the_device(cuda):
+    # a space-charge step then a push: the field left on the device and the
+    # host field of the reference's API give the same map, hence the same bits
+    torch = cuda
+    from pypatools_b200 import PusherGPU, IonSpecies, CompositeField, Field
+    from pypatools_b200.space_charge import PoissonSolverConfig, SpaceChargeSolver
+    rng = np.random.default_rng(21)
+    extent, cells = (0.02, 0.02, 0.06), (16, 16, 48)
+    n = 4000
+    p = np.column_stack([rng.normal(0, 1.5e-3, n), rng.normal(0, 1.5e-3, n), rng.normal(0, 5e-3, n)])
+    v = np.column_stack([rng.normal(0, 1e4, n), rng.normal(0, 1e4, n), np.full(n, 1.0e6)])
+    q = np.full(n, 1.602176634e-19 * 1e6)
+    solver = SpaceChargeSolver(PoissonSolverConfig(extent, cells, solver_tol=1e-10))
+    phi_h, _ = solver.solve(p, q)
+    phi_d, e_dev = solver.solve_field_device(torch.from_numpy(p).cuda(), torch.from_numpy(q).cuda())
+    assert phi_d.is_cuda and e_dev._field["z"]._values.is_cuda
+    # two solves differ only by the deposition's float64 atomics order
+    np.testing.assert_allclose(phi_d.cpu().numpy(), phi_h, rtol=0, atol=1e-12 * np.abs(phi_h).max())
+    # the same node values through the host (numpy) and the device (tensor) paths
+    e_host = Field.from_arrays(dict(zip("xyz", solver.cell_centres())),
+                               {c: e_dev._field[c]._values.cpu().numpy() for c in "xyz"})
+    b = Field(dim=0, field={"x": 0.0, "y": 0.0, "z": 0.5})
+    ion = IonSpecies("proton")
+    out = []
+    for e in (e_host, e_dev):
+        rh, vh, _ = PusherGPU(ion, "boris").track_batch(p, v, CompositeField([e], [1.0]), b, 300, 1e-10, 100)
+        out.append((rh, vh))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert np.abs(out[0][1][-1] - out[0][1][0]).max() > 0.0      # the space-charge kick is there
+    # the device field's node values changed in place count as a new field
+    pusher = PusherGPU(ion, "boris")
+    comp = CompositeField([e_dev], [1.0])
+    rh1, _, _ = pusher.track_batch(p, v, comp, b, 300, 1e-10, 100)
+    np.testing.assert_array_equal(rh1, out[1][0])
+    e_dev._field["z"]._values.mul_(2.0)
+    rh2, _, _ = pusher.track_batch(p, v, comp, b, 300, 1e-10, 100)
+    assert not np.array_equal(rh2, rh1)
