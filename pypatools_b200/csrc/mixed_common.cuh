@@ -16,6 +16,21 @@
 
 namespace ppt {
 
+// Packed float32 pairs (sm_100 FFMA2 and the f32x2 subtract): one
+// instruction issues both lanes, and each lane is rounded exactly as the
+// scalar operation, so a pair computes the same bits as two scalar
+// operations.  The trilinear interpolation of two record components at once
+// goes through these (half the issue slots of the scalar form).
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
 struct GridF {
     double lo[3];
     double d[3];

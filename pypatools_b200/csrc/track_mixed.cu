@@ -34,6 +34,23 @@ struct MixCtx {
 // its map are ~100 steps; longer launches compute the same values directly.
 constexpr int kRfTable = 512;
 
+// Components a record layout can make non-zero: bit a of e_bits (b_bits)
+// is E_a (B_a); the six-component layout also carries the constant parts.
+// x * 0 and x + 0 are not identities in IEEE arithmetic (NaN, signed
+// zeros), so the compiler keeps every operation on a component that is
+// zero by construction unless the code leaves it out: the Boris kernels
+// below do, at compile time, from these masks.
+constexpr int e_bits(int L) { return L & 7; }
+constexpr int b_bits(int L) { return (L >> 3) & 7; }
+constexpr bool bit(int m, int a) { return ((m >> a) & 1) != 0; }
+// components of p x q that can be non-zero when q has the components of qm
+constexpr int cross_bits(int qm) {
+    return ((bit(qm, 1) || bit(qm, 2)) ? 1 : 0) | ((bit(qm, 2) || bit(qm, 0)) ? 2 : 0) |
+           ((bit(qm, 0) || bit(qm, 1)) ? 4 : 0);
+}
+// velocity components a Boris step can change under layout L
+constexpr int boris_bits(int L) { return e_bits(L) | cross_bits(b_bits(L)); }
+
 // (cos, sin) of g omega dt in float64: the per-step factor of the RF phase,
 // the same for every particle, so a block tabulates it once per launch.
 __device__ __forceinline__ void rf_turn(int64_t g, double wdt, double& cg, double& sg) {
@@ -79,12 +96,22 @@ __device__ __forceinline__ void ldg_f32x8(const float* p, float (&v)[8]) {
 }
 
 // One component from 8 corners (corner q = di*4 + dj*2 + dk), x first, then
-// y, then z (interpolators.py:127-135).
+// y, then z (interpolators.py:127-135), each lerp a + t (b - a).
 template <typename Get>
 __device__ __forceinline__ float tri8(Get get, float tx, float ty, float tz) {
     float c00 = lerp_f(get(0), get(4), tx), c01 = lerp_f(get(1), get(5), tx);
     float c10 = lerp_f(get(2), get(6), tx), c11 = lerp_f(get(3), get(7), tx);
     return lerp_f(lerp_f(c00, c10, ty), lerp_f(c01, c11, ty), tz);
+}
+
+// The same for two components at once, lane by lane (packed pairs: one
+// issue slot per lerp step for both, each lane rounded as tri8 rounds).
+__device__ __forceinline__ float2 lerp2(float2 a, float2 b, float2 t) { return fma2(t, sub2(b, a), a); }
+
+__device__ __forceinline__ float2 tri8_pair(const float2 q[8], float2 tx, float2 ty, float2 tz) {
+    const float2 c00 = lerp2(q[0], q[4], tx), c01 = lerp2(q[1], q[5], tx);
+    const float2 c10 = lerp2(q[2], q[6], tx), c11 = lerp2(q[3], q[7], tx);
+    return lerp2(lerp2(c00, c10, ty), lerp2(c01, c11, ty), tz);
 }
 
 // Trilinear E/B at (cell, offset) from the float32 map of record layout L;
@@ -108,11 +135,7 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     if (!mixed_axis(cell[1], f[1], P.G.n[1], j, ty)) return false;
     if (!mixed_axis(cell[2], f[2], P.G.n[2], k, tz)) return false;
     const MapDev& m = P.map;
-    // Trilinear weights of the 8 corners (corner q = di*4 + dj*2 + dk); each
-    // component is then one product and seven FMAs.
-    const float ux = 1.0f - tx, uy = 1.0f - ty, uz = 1.0f - tz;
-    const float a00 = ux * uy, a01 = ux * ty, a10 = tx * uy, a11 = tx * ty;
-    const float w[8] = {a00 * uz, a00 * tz, a01 * uz, a01 * tz, a10 * uz, a10 * tz, a11 * uz, a11 * tz};
+    const float2 tx2 = make_float2(tx, tx), ty2 = make_float2(ty, ty), tz2 = make_float2(tz, tz);
     constexpr int W = layout_width(L);
     // corner (di, dj) = (0,0) (0,1) (1,0) (1,1); the k+1 corner is the next
     // record; 32-bit offsets when the map's elements allow (maps below 2^31
@@ -134,62 +157,58 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     }
     const float* p11 = p01 + (p10 - p00);
     const float* pc[4] = {p00, p01, p10, p11};
+    // Components adjacent in the record are interpolated as packed pairs
+    // (tri8_pair); a lone component takes tri8, the same operations.
     if constexpr (L == kLayFull) {
-        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner
+        // [Ex Ey Ez 0 | Bx By Bz 0]: one 256-bit load per corner, four pairs
         float q[8][8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             ldg_f32x8(pc[c], q[2 * c]);
             ldg_f32x8(pc[c] + 8, q[2 * c + 1]);
         }
-        float acc[6];
+        float2 o[4];
 #pragma unroll
-        for (int comp = 0; comp < 6; ++comp) {
-            const int slot = comp < 3 ? comp : comp + 1;
-            float s = w[0] * q[0][slot];
+        for (int h = 0; h < 4; ++h) {
+            float2 qp[8];
 #pragma unroll
-            for (int c = 1; c < 8; ++c) s = fmaf(w[c], q[c][slot], s);
-            acc[comp] = s;
+            for (int c = 0; c < 8; ++c) qp[c] = make_float2(q[c][2 * h], q[c][2 * h + 1]);
+            o[h] = tri8_pair(qp, tx2, ty2, tz2);
         }
-        E = E + f3(acc[0], acc[1], acc[2]);
-        B = B + f3(acc[3], acc[4], acc[5]);
+        E = E + f3(o[0].x, o[0].y, o[1].x);
+        B = B + f3(o[2].x, o[2].y, o[3].x);
     } else if constexpr (W == 4) {
-        // three packed components and a pad: one 128-bit load per corner
+        // three packed components and a pad: one 128-bit load per corner, two pairs
         float4 q[8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             q[2 * c] = __ldg(reinterpret_cast<const float4*>(pc[c]));
             q[2 * c + 1] = __ldg(reinterpret_cast<const float4*>(pc[c] + 4));
         }
-        float o0 = w[0] * q[0].x, o1 = w[0] * q[0].y, o2 = w[0] * q[0].z;
+        float2 qa[8], qb[8];
 #pragma unroll
-        for (int c = 1; c < 8; ++c) {
-            o0 = fmaf(w[c], q[c].x, o0);
-            o1 = fmaf(w[c], q[c].y, o1);
-            o2 = fmaf(w[c], q[c].z, o2);
+        for (int c = 0; c < 8; ++c) {
+            qa[c] = make_float2(q[c].x, q[c].y);
+            qb[c] = make_float2(q[c].z, q[c].w);
         }
-        if constexpr (L == kLayE) E = f3(o0, o1, o2);
-        else if constexpr (L == kLayB) B = f3(o0, o1, o2);
+        const float2 oa = tri8_pair(qa, tx2, ty2, tz2), ob = tri8_pair(qb, tx2, ty2, tz2);
+        if constexpr (L == kLayE) E = f3(oa.x, oa.y, ob.x);
+        else if constexpr (L == kLayB) B = f3(oa.x, oa.y, ob.x);
         else {   // kLayExEyBz
-            E = f3(o0, o1, 0.0f);
-            B = f3(0.0f, 0.0f, o2);
+            E = f3(oa.x, oa.y, 0.0f);
+            B = f3(0.0f, 0.0f, ob.x);
         }
     } else if constexpr (W == 2) {
-        // kLayEzBz: one 64-bit load per corner
+        // kLayEzBz: one 64-bit load per corner, one pair
         float2 q[8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             q[2 * c] = __ldg(reinterpret_cast<const float2*>(pc[c]));
             q[2 * c + 1] = __ldg(reinterpret_cast<const float2*>(pc[c] + 2));
         }
-        float o0 = w[0] * q[0].x, o1 = w[0] * q[0].y;
-#pragma unroll
-        for (int c = 1; c < 8; ++c) {
-            o0 = fmaf(w[c], q[c].x, o0);
-            o1 = fmaf(w[c], q[c].y, o1);
-        }
-        E = f3(0.0f, 0.0f, o0);
-        B = f3(0.0f, 0.0f, o1);
+        const float2 o = tri8_pair(q, tx2, ty2, tz2);
+        E = f3(0.0f, 0.0f, o.x);
+        B = f3(0.0f, 0.0f, o.y);
     } else {
         // kLayBz: one 32-bit load per corner
         float q[8];
@@ -198,10 +217,7 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
             q[2 * c] = __ldg(pc[c]);
             q[2 * c + 1] = __ldg(pc[c] + 1);
         }
-        float o = w[0] * q[0];
-#pragma unroll
-        for (int c = 1; c < 8; ++c) o = fmaf(w[c], q[c], o);
-        B = f3(0.0f, 0.0f, o);
+        B = f3(0.0f, 0.0f, tri8([&](int c) { return q[c]; }, tx, ty, tz));
     }
     return true;
 }
@@ -221,7 +237,8 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
     bool in = gather_mixed<L>(*c.P, cell, f, E, B);
     c.hits += in;
     if (RF) {
-        if (E.x != 0.0f || E.y != 0.0f || E.z != 0.0f) {
+        constexpr int EM = e_bits(L);
+        if ((bit(EM, 0) && E.x != 0.0f) || (bit(EM, 1) && E.y != 0.0f) || (bit(EM, 2) && E.z != 0.0f)) {
             // omega (t0 + g dt + toff) + phi_i = (omega t0 + phi_i) + g (omega dt) + omega toff, in float64
             float cf;
             if (toff == 0.0) {
@@ -235,23 +252,66 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
                 const double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
                 cf = cosf((float)red);
             }
-            E = cf * E;
+            if constexpr (bit(EM, 0)) E.x = cf * E.x;
+            if constexpr (bit(EM, 1)) E.y = cf * E.y;
+            if constexpr (bit(EM, 2)) E.z = cf * E.z;
         }
     }
     return in || const_fields<L>(*c.P);
 }
 
 // Boris velocity increment in float32 (pusher.py:149-163 rearranged):
-// v_new - v = 2 a + (v- + v- x t) x s,  a = (q/m) E dt/2,  v- = v + a.
+// v_new - v = 2 a + (v- + v- x t) x s,  a = (q/m) E dt/2,  v- = v + a,
+// t = (q/m) B dt/2, s = 2 t / (1 + t.t), with the components outside EM
+// (E) and BM (B) left out; the components of the result outside
+// e_bits | cross_bits(BM) are zero.
+template <int QM, int I>
+__device__ __forceinline__ float cross_m(const float p[3], const float q[3]) {
+    // (p x q)_I without q's zero components (crossf's form when both terms are there)
+    constexpr int J = (I + 1) % 3, K = (I + 2) % 3;
+    if constexpr (bit(QM, K) && bit(QM, J)) return fmaf(p[J], q[K], -p[K] * q[J]);
+    else if constexpr (bit(QM, K)) return p[J] * q[K];
+    else if constexpr (bit(QM, J)) return -(p[K] * q[J]);
+    else return 0.0f;
+}
+
+template <int M>
+__device__ __forceinline__ float self_dot_m(const float t[3]) {
+    // dotf(t, t) without the zero components (z, then y, then x)
+    float acc = 0.0f;
+    if constexpr (bit(M, 2)) acc = t[2] * t[2];
+    if constexpr (bit(M, 1)) acc = bit(M, 2) ? fmaf(t[1], t[1], acc) : t[1] * t[1];
+    if constexpr (bit(M, 0)) acc = (bit(M, 1) || bit(M, 2)) ? fmaf(t[0], t[0], acc) : t[0] * t[0];
+    return acc;
+}
+
+template <int EM, int BM>
+__device__ __forceinline__ F3 boris_dv_m(F3 vv, F3 E, F3 B, float hqdt) {
+    constexpr int CM = cross_bits(BM);
+    const float v[3] = {vv.x, vv.y, vv.z}, e[3] = {E.x, E.y, E.z}, b[3] = {B.x, B.y, B.z};
+    float a[3], vm[3], t[3], s[3], vp[3], dv[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        a[i] = bit(EM, i) ? hqdt * e[i] : 0.0f;
+        vm[i] = bit(EM, i) ? v[i] + a[i] : v[i];
+        t[i] = bit(BM, i) ? hqdt * b[i] : 0.0f;
+    }
+    const float s_f = __fdividef(2.0f, 1.0f + self_dot_m<BM>(t));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) s[i] = bit(BM, i) ? s_f * t[i] : 0.0f;
+    vp[0] = bit(CM, 0) ? vm[0] + cross_m<BM, 0>(vm, t) : vm[0];
+    vp[1] = bit(CM, 1) ? vm[1] + cross_m<BM, 1>(vm, t) : vm[1];
+    vp[2] = bit(CM, 2) ? vm[2] + cross_m<BM, 2>(vm, t) : vm[2];
+    const float c2[3] = {cross_m<BM, 0>(vp, s), cross_m<BM, 1>(vp, s), cross_m<BM, 2>(vp, s)};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        dv[i] = bit(EM, i) ? (bit(CM, i) ? fmaf(2.0f, a[i], c2[i]) : 2.0f * a[i]) : (bit(CM, i) ? c2[i] : 0.0f);
+    return f3(dv[0], dv[1], dv[2]);
+}
+
+template <int L>
 __device__ __forceinline__ F3 boris_dv(F3 v, F3 E, F3 B, float hqdt) {
-    F3 a = hqdt * E;
-    F3 vm = v + a;
-    F3 t = hqdt * B;
-    float s_f = __fdividef(2.0f, 1.0f + dotf(t, t));
-    F3 s = s_f * t;
-    F3 vp = vm + crossf(vm, t);
-    F3 c2 = crossf(vp, s);
-    return f3(fmaf(2.0f, a.x, c2.x), fmaf(2.0f, a.y, c2.y), fmaf(2.0f, a.z, c2.z));
+    return boris_dv_m<e_bits(L), b_bits(L)>(v, E, B, hqdt);
 }
 
 constexpr float kCf = 299792458.0f;
@@ -312,11 +372,16 @@ __device__ __forceinline__ void vel_add(float vh[3], float vl[3], F3 d) {
 // part and for the rotation to first order (the neglected part is ~ t^2 of
 // the correction); d ws is below half an ulp of d, so it goes into the low
 // word, and costs three FMAs off the step's critical path.
+// (Components outside the mask M stay unchanged: d is zero there.)
+template <int M>
 __device__ __forceinline__ void vel_add_boris(float vh[3], float vl[3], F3 d, float ws) {
-    vel_add(vh, vl, d);
-    vl[0] = fmaf(d.x, ws, vl[0]);
-    vl[1] = fmaf(d.y, ws, vl[1]);
-    vl[2] = fmaf(d.z, ws, vl[2]);
+    const float dd[3] = {d.x, d.y, d.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (!bit(M, a)) continue;
+        ff_add(vh[a], vl[a], dd[a]);
+        vl[a] = fmaf(dd[a], ws, vl[a]);
+    }
 }
 
 // The same for the Boris steps of a track, at a third of the cost: a fast
@@ -327,10 +392,12 @@ __device__ __forceinline__ void vel_add_boris(float vh[3], float vl[3], F3 d, fl
 // (g + 1) % 4 == 0 that see a field, so the low word stays within a few ulps
 // of the high one and a track's bits do not depend on how it is split into
 // launches.  vh + vl stays the accumulated velocity throughout.
+template <int M>
 __device__ __forceinline__ void vel_add_fast(float vh[3], float vl[3], F3 d, float ws) {
     const float dd[3] = {d.x, d.y, d.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+        if (!bit(M, a)) continue;
         const float s = vh[a] + dd[a];
         const float err = dd[a] - (s - vh[a]);
         vl[a] = fmaf(dd[a], ws, vl[a] + err);
@@ -338,9 +405,11 @@ __device__ __forceinline__ void vel_add_fast(float vh[3], float vl[3], F3 d, flo
     }
 }
 
+template <int M>
 __device__ __forceinline__ void vel_renorm(float vh[3], float vl[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+        if (!bit(M, a)) continue;
         const float s = vh[a] + vl[a];
         vl[a] = vl[a] - (s - vh[a]);
         vh[a] = s;
@@ -375,10 +444,12 @@ __device__ __forceinline__ void offset_point(const TrackMixDev& P, const int cel
 
 // Per-step position increment v dt / d in cell units as a float-float pair,
 // recomputed only when the velocity changes.
+template <int M = 7>
 __device__ __forceinline__ void increment(const TrackMixDev& P, const float vh[3], const float vl[3], float dh[3],
                                           float dl[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
+        if (!bit(M, a)) continue;
         float p = vh[a] * P.kh[a];
         float e = fmaf(vh[a], P.kh[a], -p);
         dh[a] = p;
@@ -487,12 +558,15 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], f
         if (fields_mixed<RF, L>(c, cell, fn, g, 0.0, E, B)) {
             F3 v = f3(vh[0], vh[1], vh[2]);
             if constexpr (ALG == PPT_ALG_BORIS) {
-                vel_add_fast(vh, vl, boris_dv(v, E, B, P.hqdt), P.wscale);
-                if (((unsigned)(g + 1) & 3u) == 0u) vel_renorm(vh, vl);
+                // only the velocity components the layout's fields can change
+                constexpr int DM = boris_bits(L);
+                vel_add_fast<DM>(vh, vl, boris_dv<L>(v, E, B, P.hqdt), P.wscale);
+                if (((unsigned)(g + 1) & 3u) == 0u) vel_renorm<DM>(vh, vl);
+                increment<DM>(P, vh, vl, d.dh, d.dl);
             } else {
                 vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
+                increment(P, vh, vl, d.dh, d.dl);
             }
-            increment(P, vh, vl, d.dh, d.dl);
         }
         // where fields act (or may), the full float-float increment and a carry
 #pragma unroll
@@ -623,7 +697,8 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 F3 E, B;
                 if (fields_mixed<RF, L>(c, cell, f, P.step0, 0.0, E, B))
                     // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
-                    vel_add_boris(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt), P.wscale);
+                    vel_add_boris<boris_bits(L)>(vh, vl, boris_dv<L>(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt),
+                                                 P.wscale);
             }
             if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
         }
@@ -719,7 +794,8 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 }
                 if (fields_mixed<RF, L>(c, cn, fn, P.nsteps_total, 0.0, E, B))
                     // Boris push with time step +dt/2 (pusher.py:993-1007)
-                    vel_add_boris(vh, vl, boris_dv(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt), P.wscale);
+                    vel_add_boris<boris_bits(L)>(vh, vl, boris_dv<L>(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt),
+                                                 P.wscale);
                 if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
             }
         }

@@ -1,9 +1,13 @@
 """Maps that store only the components that are not identically zero.
 
 A component that is zero in every term contributes exact zeros to the
-interpolation, so a map without it must give the same bits as a map that
-stores it: both forms are compared bitwise against maps of the full
-E / B / E+B records, for every compiled layout."""
+interpolation, so in the float64 form a map without it must give the same
+bits as a map that stores it: compared bitwise against maps of the full
+E / B / E+B records, for every compiled layout.  The mixed form's Boris
+kernels of a pruned layout also leave the zero components' products out of
+the rotation (the full-record kernels evaluate them, and the compiler fuses
+the remaining products differently), so there the two agree to float32
+rounding: within 1e-6 relative."""
 import ctypes
 
 import numpy as np
@@ -59,8 +63,15 @@ def test_pruned_maps_are_bitwise_equal_to_full_maps(cuda, precision, case):
         assert df.layouts == [layout], (name, df.layouts)
         full, rh0, vh0 = _track(wl, e, b, precision, False, alg, omega, phase)
         assert full.layouts[0] in (0x07, 0x38, 0x3F) and full.map_bytes >= df.map_bytes
-        np.testing.assert_array_equal(rh, rh0, err_msg=f"{name} {alg} r")
-        np.testing.assert_array_equal(vh, vh0, err_msg=f"{name} {alg} v")
+        if precision == "fp64":
+            np.testing.assert_array_equal(rh, rh0, err_msg=f"{name} {alg} r")
+            np.testing.assert_array_equal(vh, vh0, err_msg=f"{name} {alg} v")
+        else:
+            assert np.array_equal(np.isnan(rh), np.isnan(rh0)), (name, alg)
+            fin = ~np.isnan(rh0[..., 0])
+            dr = np.linalg.norm(rh - rh0, axis=-1)[fin] / np.maximum(np.linalg.norm(rh0, axis=-1)[fin], 0.05)
+            dv = np.linalg.norm(vh - vh0, axis=-1)[fin] / np.linalg.norm(vh0, axis=-1)[fin]
+            assert dr.max() <= 1e-6 and dv.max() <= 1e-6, (name, alg, dr.max(), dv.max())
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
