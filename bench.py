@@ -66,7 +66,7 @@ def parse():
 # DRAM bytes per particle per launch of the mixed track kernel, from the ncu
 # capture of a 100-step in-map launch on the RF-gap workload at 1e6 protons
 # (the state read and written; the map's occupied cells stay in L1/L2).
-MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 65.5
+MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 65.2
 
 
 def _timed_track(tr, r0, v0, nsteps, sort_every, phase=None):
@@ -651,7 +651,7 @@ def main():
                 "note": "algorithmic bytes as defined for this path count every corner gather of the "
                         "stored components, but the gathers of cell-sorted particles are served from L1 "
                         "and the DRAM traffic is the state in and out (traffic); the kernel is not "
-                        "HBM-bound: ncu shows it issue-bound in the map (91 % issue-active, 240 "
+                        "HBM-bound: ncu shows it issue-bound in the map (86 % issue-active, 205 "
                         "warp-instructions per warp-step)"}
 
     # e2e through the public API with host buffers (H2D of r0/v0/phase, D2H of the histories)
