@@ -355,8 +355,8 @@ def load_aima_agora(path, mirror=False, interp_resolution=1000):
         raise FileNotFoundError(f"Path not found: {path}")
     try:
         names = [e.name for e in os.scandir(directory) if e.is_file() and e.name.endswith(".map")]
-    except Exception as exc:
-        raise RuntimeError(f"Error scanning directory: {exc}")
+    except OSError as exc:
+        raise RuntimeError(f"Error scanning directory: {exc}") from exc
     if not names:
         raise FileNotFoundError(f"No .map files found in {directory}")
     files = []   # (path, component, z [mm])
@@ -367,7 +367,7 @@ def load_aima_agora(path, mirror=False, interp_resolution=1000):
             if comp not in ("br", "bf", "bz"):
                 continue
             files.append((os.path.join(directory, name), comp, float(z_text)))
-        except Exception:
+        except (IndexError, ValueError):   # not named <...>Z<z>-<component>.map
             continue
     if not files:
         raise ValueError("No valid .map files found")

@@ -348,7 +348,9 @@ class HostStager:
 
     def copy(self, src, dst, after=None):
         """Queue the copy of the contiguous device tensor ``src`` into the
-        contiguous numpy array ``dst`` (same bytes), after event ``after``."""
+        contiguous numpy array ``dst`` (same bytes), after event ``after``.
+        The caller keeps ``src`` alive (and unchanged) until ``finish()``
+        returns: the copy stream reads it after this call returns."""
         with self.lock:
             self._copy(src, dst, after)
 

@@ -203,3 +203,21 @@ def test_gpu_from_file_midplane_evaluates(cuda, cases):
     pts = np.random.default_rng(2).uniform(-0.2, 0.2, (2000, 3))
     ref = orc.MapField((gx, gy), {"x": None, "y": None, "z": G["opal/values/z"]})(pts)
     np.testing.assert_allclose(f(pts), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
+def test_aima_directory_checks(tmp_path):
+    # field_loaders.py's AIMA reader: files not named <...>Z<z>-<br|bf|bz>.map
+    # are skipped; none left, or components on different z sets, is an error
+    # (raised before any resampling)
+    d = tmp_path / "aima"
+    d.mkdir()
+    for junk in ("notes.map", "fieldZabc-br.map", "fieldZ010-bx.map", "field-Z.map"):
+        (d / junk).write_text("x\n")
+    with pytest.raises(ValueError, match="No valid .map files"):
+        loaders.load_aima_agora(str(d))
+    for name in ("fieldZ000-br.map", "fieldZ000-bf.map", "fieldZ000-bz.map", "fieldZ010-br.map"):
+        (d / name).write_text("x\n")
+    with pytest.raises(ValueError, match="same z positions"):
+        loaders.load_aima_agora(str(d))
+    with pytest.raises(FileNotFoundError):
+        loaders.load_aima_agora(str(tmp_path / "missing"))
