@@ -101,6 +101,24 @@ class PoissonSolverConfig:
         self.interpolator_backend = interpolator_backend
 
 
+def check_device_inputs(particles, charges, device):
+    """(particles, charges) as the deposit kernel reads them: float64 tensors
+    on ``device``, (M, 3) row-major and (M,), contiguous.  Anything else is
+    refused here (a float32 or host array would be read past its end)."""
+    import torch
+    if not (torch.is_tensor(particles) and torch.is_tensor(charges)):
+        raise TypeError("particles and charges must be torch tensors on the solver's device "
+                        "(solve() takes numpy arrays)")
+    if particles.dtype != torch.float64 or charges.dtype != torch.float64:
+        raise TypeError(f"particles and charges must be float64, got {particles.dtype} and {charges.dtype}")
+    if particles.dim() != 2 or particles.shape[1] != 3 or tuple(charges.shape) != (particles.shape[0],):
+        raise ValueError(f"particles must be (M, 3) and charges (M,), got {tuple(particles.shape)} and "
+                         f"{tuple(charges.shape)}")
+    if particles.device != device or charges.device != device:
+        raise ValueError(f"particles and charges must be on {device}, got {particles.device} and {charges.device}")
+    return particles.contiguous(), charges.contiguous()
+
+
 class SpaceChargeSolver:
     """GPU counterpart of ``PyAMGPoissonSolver`` (conductor cells from an
     optional electrode assembly)."""
@@ -174,6 +192,7 @@ class SpaceChargeSolver:
         ``self.phi`` and (Ex, Ey, Ez) in ``self.e``; returns them.  Everything
         runs on ``stream`` (default: the current stream)."""
         import torch
+        particles, charges = check_device_inputs(particles, charges, self._rho.device)
         if stream is not None:
             with torch.cuda.stream(stream):
                 return self.solve_device(particles, charges)

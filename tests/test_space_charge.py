@@ -61,6 +61,30 @@ def test_poisson_argument_checks_without_gpu():
     assert b"positive" in lib.ppt_last_error()
 
 
+def test_device_solve_input_checks_without_gpu():
+    # the deposit kernel reads (M, 3) float64 rows: anything else is refused
+    # on the host before a launch
+    import torch
+    from pypatools_b200.space_charge import check_device_inputs
+    dev = torch.device("cpu")
+    p, q = torch.zeros((5, 3), dtype=torch.float64), torch.zeros(5, dtype=torch.float64)
+    a, b = check_device_inputs(p, q, dev)
+    assert a.is_contiguous() and b.shape == (5,)
+    a, _ = check_device_inputs(torch.zeros((3, 5), dtype=torch.float64).t(), q, dev)   # made contiguous
+    assert a.is_contiguous() and a.shape == (5, 3)
+    with pytest.raises(TypeError, match="torch tensors"):
+        check_device_inputs(np.zeros((5, 3)), q, dev)
+    with pytest.raises(TypeError, match="float64"):
+        check_device_inputs(p.float(), q, dev)
+    with pytest.raises(ValueError, match=r"\(M, 3\)"):
+        check_device_inputs(torch.zeros((5, 2), dtype=torch.float64), q, dev)
+    with pytest.raises(ValueError, match=r"\(M, 3\)"):
+        check_device_inputs(p, torch.zeros(4, dtype=torch.float64), dev)
+    with pytest.raises(ValueError, match="must be on"):
+        check_device_inputs(p, q, torch.device("cuda", 0))
+    check_device_inputs(torch.zeros((0, 3), dtype=torch.float64), torch.zeros(0, dtype=torch.float64), dev)
+
+
 def _cond():
     cells = tuple(int(c) for c in G["cond/cells"])
     h = [G["cond/extent"][a] / cells[a] for a in range(3)]
