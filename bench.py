@@ -154,8 +154,8 @@ def run_sector_ring(args, dev):
     qm = wl.species.q_over_m
     out = {}
     dfm = DeviceFields(None, bf, "mixed", dev)
-    warm = DeviceTracker("boris", qm, dfm, 4096, 50, wl.dt, 50, "mixed", device=dev)
-    _timed_track(warm, r0[:4096], v0[:4096], 50, args.sort_every)
+    warm = DeviceTracker("boris", qm, dfm, min(wl.n, 4096), 50, wl.dt, 50, "mixed", device=dev)
+    _timed_track(warm, r0[:warm.n], v0[:warm.n], 50, args.sort_every)
     tr = DeviceTracker("boris", qm, dfm, wl.n, wl.nsteps, wl.dt, wl.rec_every, "mixed", device=dev)
     ms = _timed_track(tr, r0, v0, wl.nsteps, args.sort_every)
     out["mixed"] = {"particle_steps_per_s": wl.n * wl.nsteps / (ms / 1e3), "ms_job": ms}

@@ -67,6 +67,22 @@ def default_steps_per_launch(n, nsteps):
     return int(max(1, min(nsteps, 2 ** 31 - 1, math.ceil(4e9 / max(n, 1)))))
 
 
+def check_rows(t, n, device, name):
+    """``t`` as the state load / store kernels read and write it: a
+    contiguous (n, 3) float64 tensor on ``device`` (a CUDA device with its
+    index).  Anything else is refused before a launch: the kernels address n
+    rows of 24 B from its data pointer."""
+    import torch
+    if not torch.is_tensor(t):
+        raise TypeError(f"{name} must be a torch tensor, got {type(t).__name__}")
+    if t.dtype != torch.float64 or tuple(t.shape) != (n, 3):
+        raise ValueError(f"{name} must be a ({n}, 3) float64 tensor, got {tuple(t.shape)} {t.dtype}")
+    if t.device != device or not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous on {device} (got {t.device}, "
+                         f"{'contiguous' if t.is_contiguous() else 'strided'})")
+    return t
+
+
 class DeviceTracker:
     """Device-resident state of one bunch: the building block of
     ``track_batch``, the serving loop and the benchmark.
@@ -140,6 +156,8 @@ class DeviceTracker:
             ph = torch.as_tensor(rf_phase, dtype=torch.float64)
             if ph.ndim == 0:
                 ph = ph.expand(n)
+            if tuple(ph.shape) != (n,):
+                raise ValueError(f"rf_phase must be a scalar or ({n},), got {tuple(ph.shape)}")
             self.rf_phase = ph.to(dev).contiguous().clone()
         else:
             self.rf_phase = None
@@ -154,6 +172,9 @@ class DeviceTracker:
 
     def load(self, r, v, stream=None):
         """r, v: (n,3) float64 CUDA tensors."""
+        dev = self.status.device
+        check_rows(r, self.n, dev, "r")
+        check_rows(v, self.n, dev, "v")
         _lib.check(self.lib.ppt_state_load(self.state, self.dfields.fields, r.data_ptr(), v.data_ptr(),
                                            self._stream(stream)))
         self.launches += 1
@@ -287,6 +308,9 @@ class DeviceTracker:
 
     def store(self, r, v, stream=None):
         """Write the current state as (n,3) float64 r, v in row order."""
+        for t, name in ((r, "r"), (v, "v")):
+            if t is not None:
+                check_rows(t, self.n, self.status.device, name)
         _lib.check(self.lib.ppt_state_store(self.state, self.dfields.fields,
                                             self.order.data_ptr() if self.order is not None else None,
                                             r.data_ptr() if r is not None else None,

@@ -175,3 +175,23 @@ def test_pusher_constructor_mirrors_reference():
         PusherGPU(ion, "boris", electrode_assembly=object())
     p.change_algorithm("boris")
     assert p.algorithm == "boris" and "PusherGPU(ion=proton" in repr(p)
+
+
+def test_state_rows_are_checked_before_a_launch():
+    # the state load / store kernels address n rows of 24 B: the tracker
+    # refuses anything else on the host
+    import torch
+    from pypatools_b200.pusher import check_rows
+    dev = torch.device("cpu")
+    r = torch.zeros((4, 3), dtype=torch.float64)
+    assert check_rows(r, 4, dev, "r") is r
+    with pytest.raises(TypeError):
+        check_rows(np.zeros((4, 3)), 4, dev, "r")
+    with pytest.raises(ValueError, match=r"\(4, 3\) float64"):
+        check_rows(r[:3], 4, dev, "r")
+    with pytest.raises(ValueError, match=r"\(4, 3\) float64"):
+        check_rows(r.float(), 4, dev, "r")
+    with pytest.raises(ValueError, match="strided"):
+        check_rows(torch.zeros((3, 4), dtype=torch.float64).t(), 4, dev, "r")
+    with pytest.raises(ValueError, match="contiguous on cuda:0"):
+        check_rows(r, 4, torch.device("cuda", 0), "r")
