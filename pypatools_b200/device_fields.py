@@ -46,6 +46,23 @@ class _MapTerm:
         self.scale = scale          # float
 
 
+def check_term_sizes(term):
+    """Every component of a map term holds one value per grid node: the map
+    add kernel reads that many from each component's data pointer, so a
+    shorter array (an interpolator built elsewhere, a mutated tensor) is
+    refused here instead of read past its end."""
+    nodes = 1
+    for axis in term.grid:
+        nodes *= int(np.asarray(axis).shape[0])
+    for c, a in term.comps.items():
+        if a is None:
+            continue
+        size = int(a.numel()) if _is_tensor(a) else int(np.asarray(a).size)
+        if size != nodes:
+            dims = " x ".join(str(int(np.asarray(ax).shape[0])) for ax in term.grid)
+            raise ValueError(f"field component {c!r} has {size} node values, its grid {dims} = {nodes} nodes")
+
+
 class FieldTerms:
     """A field as (constant vector, list of map terms)."""
 
@@ -262,6 +279,7 @@ class DeviceFields:
 
     def _add_term(self, lib, handle, kind, term, stream, mask):
         torch = self._torch
+        check_term_sizes(term)
         ptrs = (_lib.c_void_p * 6)()
         scales = (_lib.c_double * 6)()
         base = 0 if kind == "e" else 3

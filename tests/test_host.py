@@ -119,6 +119,8 @@ def test_decompose_reference_duck_types():
     f3 = _FakeRefField(3, {c: _FakeNumbaInterp(g, v) for c in "xyz"}, scaling=2.0)
     t = decompose(f3)
     assert len(t.terms) == 1 and t.terms[0].scale == 2.0 and not t.const.any()
+    from pypatools_b200.device_fields import check_term_sizes
+    check_term_sizes(t.terms[0])
     f0 = _FakeRefField(0, {"x": 1.0, "y": 2.0, "z": 3.0}, scaling=0.5)
     np.testing.assert_array_equal(decompose(f0).const, [0.5, 1.0, 1.5])
 
@@ -195,3 +197,20 @@ def test_state_rows_are_checked_before_a_launch():
         check_rows(torch.zeros((3, 4), dtype=torch.float64).t(), 4, dev, "r")
     with pytest.raises(ValueError, match="contiguous on cuda:0"):
         check_rows(r, 4, torch.device("cuda", 0), "r")
+
+
+def test_map_terms_hold_one_value_per_node():
+    # the map add kernel reads one value per grid node from each component
+    from pypatools_b200.device_fields import check_term_sizes, _MapTerm
+    g3 = {"x": np.linspace(0, 1, 4), "y": np.linspace(0, 1, 3), "z": np.linspace(0, 1, 5)}
+    f3 = Field.from_arrays(g3, {c: np.ones((4, 3, 5)) for c in "xyz"})
+    z = np.linspace(0, 1, 7)
+    f1 = Field.from_arrays({"z": z}, {c: np.ones(7) for c in "xyz"})
+    f2 = Field.from_arrays({"x": z, "y": z[:4]}, {c: np.ones((7, 4)) for c in "xyz"})
+    for f in (f3, f1, f2, 2.0 * f3 + f3):
+        for t in decompose(f).terms:
+            check_term_sizes(t)
+    t = decompose(f3).terms[0]
+    bad = _MapTerm(t.grid, {"x": np.ones(59), "y": None, "z": t.comps["z"]}, 1.0)
+    with pytest.raises(ValueError, match="59 node values, its grid 4 x 3 x 5 = 60 nodes"):
+        check_term_sizes(bad)
