@@ -264,6 +264,15 @@ def polar_to_cartesian(r_nodes, theta_nodes, comps, x, y, r_scale=1.0, want=(Tru
     at one z.  Returns [B_x, B_y, B_z] as (nx, ny) float64 arrays (None where
     ``want`` is False).  Runs ``ppt_polar_to_cartesian``."""
     import torch
+    r_nodes, theta_nodes, x, y = (np.asarray(a, dtype=np.float64) for a in (r_nodes, theta_nodes, x, y))
+    if any(a.ndim != 1 for a in (r_nodes, theta_nodes, x, y)):
+        raise ValueError("r_nodes, theta_nodes, x and y must be 1D")
+    if len(comps) != 3 or len(want) != 3:
+        raise ValueError("comps and want hold the (r, theta, z) components: three entries each")
+    for c in comps:
+        if c is not None and np.shape(c) != (r_nodes.shape[0], theta_nodes.shape[0]):
+            raise ValueError(f"a component of shape {np.shape(c)} on a ({r_nodes.shape[0]}, "
+                             f"{theta_nodes.shape[0]}) (r, theta) node grid")
     if not torch.cuda.is_available():
         raise RuntimeError("the cylindrical-map resampling runs on the GPU (no CPU fallback)")
     lib = _lib.load()

@@ -221,3 +221,15 @@ def test_aima_directory_checks(tmp_path):
         loaders.load_aima_agora(str(d))
     with pytest.raises(FileNotFoundError):
         loaders.load_aima_agora(str(tmp_path / "missing"))
+
+
+def test_polar_resample_argument_checks_without_gpu():
+    # the resampling kernel reads nr x nt values per component: shapes are
+    # checked on the host first
+    r, th, x = np.linspace(0, 1, 4), np.linspace(0, 350, 36), np.linspace(-1, 1, 5)
+    with pytest.raises(ValueError, match=r"shape \(36, 4\) on a \(4, 36\)"):
+        loaders.polar_to_cartesian(r, th, (None, None, np.zeros((36, 4))), x, x)
+    with pytest.raises(ValueError, match="1D"):
+        loaders.polar_to_cartesian(r[None], th, (None, None, None), x, x)
+    with pytest.raises(ValueError, match="three entries"):
+        loaders.polar_to_cartesian(r, th, (None, np.zeros((4, 36))), x, x)
