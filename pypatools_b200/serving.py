@@ -44,6 +44,10 @@ class TrackingJob:
         self.precision = precision
         self.r0 = np.ascontiguousarray(r0, dtype=np.float64)
         self.v0 = np.ascontiguousarray(v0, dtype=np.float64)
+        if self.r0.ndim != 2 or self.r0.shape[1] != 3 or self.v0.shape != self.r0.shape:
+            raise ValueError(f"r0 and v0 must both be (M, 3), got {self.r0.shape} and {self.v0.shape}")
+        if int(nsteps) < 0 or (rec_every is not None and int(rec_every) < 1):
+            raise ValueError("nsteps must be >= 0 and rec_every >= 1")
         self.n = self.r0.shape[0]
         self.efield, self.bfield = efield, bfield
         self.nsteps = int(nsteps)

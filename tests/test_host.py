@@ -214,3 +214,16 @@ def test_map_terms_hold_one_value_per_node():
     bad = _MapTerm(t.grid, {"x": np.ones(59), "y": None, "z": t.comps["z"]}, 1.0)
     with pytest.raises(ValueError, match="59 node values, its grid 4 x 3 x 5 = 60 nodes"):
         check_term_sizes(bad)
+
+
+def test_tracking_job_arguments_checked_at_submission():
+    from pypatools_b200.serving import TrackingJob
+    r = np.zeros((5, 3))
+    j = TrackingJob(0, 1.0, "boris", r, r, None, None, 100, 1e-11, rec_every=10)
+    assert j.n == 5 and j.n_rec == 11
+    with pytest.raises(ValueError, match=r"\(M, 3\)"):
+        TrackingJob(0, 1.0, "boris", r, np.zeros((4, 3)), None, None, 100, 1e-11)
+    with pytest.raises(ValueError, match=r"\(M, 3\)"):
+        TrackingJob(0, 1.0, "boris", np.zeros(15), np.zeros(15), None, None, 100, 1e-11)
+    with pytest.raises(ValueError, match="rec_every"):
+        TrackingJob(0, 1.0, "boris", r, r, None, None, 100, 1e-11, rec_every=0)
