@@ -264,7 +264,7 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
 // v_new - v = 2 a + (v- + v- x t) x s,  a = (q/m) E dt/2,  v- = v + a,
 // t = (q/m) B dt/2, s = 2 t / (1 + t.t), with the components outside EM
 // (E) and BM (B) left out; the components of the result outside
-// e_bits | cross_bits(BM) are zero.
+// EM | cross_bits(BM) are zero.
 template <int QM, int I>
 __device__ __forceinline__ float cross_m(const float p[3], const float q[3]) {
     // (p x q)_I without q's zero components (crossf's form when both terms are there)
