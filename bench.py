@@ -51,8 +51,14 @@ def parse():
                     help="cell re-sort interval in steps while the map is populated (also the launch length "
                          "then); 0 = never; default 300 for rf_gap (best of a 50-1000 sweep), 100 otherwise "
                          "(the sector-ring configuration's interval)")
-    ap.add_argument("--serve-jobs", type=int, default=300,
-                    help="jobs of the serving stream per form (2000 = the full stream); 0 skips it")
+    ap.add_argument("--serve-jobs", type=int, default=2000,
+                    help="jobs of the serving stream per form (default: the whole 2000-job stream); 0 skips it")
+    ap.add_argument("--no-sweep", action="store_true",
+                    help="skip the electron pusher sweep object of the default line")
+    ap.add_argument("--no-sector-ring", action="store_true",
+                    help="skip the large-scale sector-ring object of the default line")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the deposition, space-charge, electrode and loader objects")
     args = ap.parse_args()
     defaults = {"rf_gap": (10_000_000, 20_000), "pusher_sweep": (1_000_000, 10_000),
                 "sector_ring": (100_000_000, 50_000)}[args.workload]
@@ -67,6 +73,10 @@ def parse():
 # capture of a 100-step in-map launch on the RF-gap workload at 1e6 protons
 # (the state read and written; the map's occupied cells stay in L1/L2).
 MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 65.2
+# Warp-instructions issued per warp-step (32 particle-steps) by the mixed
+# Boris kernel on the RF-gap layout, in the map and in field-free drift
+# (ncu smsp__inst_executed of one launch / warps / steps).
+WARP_INST_PER_WARP_STEP = {"map": 205.0, "drift": 13.0}
 
 
 def _timed_track(tr, r0, v0, nsteps, sort_every, phase=None):
@@ -97,29 +107,30 @@ def _rel_err(r, r64, floor):
     return {"p50": q(0.5), "p99": q(0.99), "max": float(srt[-1]), "over_1e-6": int((srt > 1e-6).sum())}
 
 
-def run_pusher_sweep(args, dev):
+def run_pusher_sweep(dev, n=1_000_000, nsteps=10_000, sort_every=100):
     """1e6 electrons (10 keV-10 MeV, isotropic) in a radial 1 MV/m E and a
     0.5 T cos(pi z / 0.2 m) solenoid B on a 129^3 map, dt = 1e-12 s, 1e4
-    steps: Boris, vay_rel and rk4_rel in both forms, the mixed form's error
-    against the float64 form (which matches the oracle to 1e-10)."""
+    steps: the reference's Boris, vay_rel and rk4_rel and the added
+    relativistic Boris and Vay (2008), each in both forms, with the mixed
+    form's error against the float64 form (which matches the oracle to 1e-10)."""
     import torch
     from pypatools_b200 import workloads, Field
     from pypatools_b200.device_fields import DeviceFields
     from pypatools_b200.pusher import DeviceTracker
-    wl = workloads.radial_e_solenoid_electrons(n=args.n, nsteps=args.nsteps)
+    wl = workloads.radial_e_solenoid_electrons(n=n, nsteps=nsteps)
     g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
     ef, bf = Field.from_arrays(g, wl.e_values), Field.from_arrays(g, wl.b_values)
     r0, v0 = torch.from_numpy(wl.r0).to(dev), torch.from_numpy(wl.v0).to(dev)
     out = {}
-    for alg in ("boris", "vay_rel", "rk4_rel"):
+    for alg in ("boris", "vay_rel", "rk4_rel", "boris_rel", "vay"):
         res, hist = {}, {}
         for form in ("fp64", "mixed"):
             df = DeviceFields(ef, bf, form, dev)
             tr = DeviceTracker(alg, wl.species.q_over_m, df, wl.n, wl.nsteps, wl.dt, wl.rec_every, form,
                                device=dev)
             warm = DeviceTracker(alg, wl.species.q_over_m, df, min(wl.n, 4096), 50, wl.dt, 50, form, device=dev)
-            _timed_track(warm, r0[:warm.n], v0[:warm.n], 50, args.sort_every)
-            ms = _timed_track(tr, r0, v0, wl.nsteps, args.sort_every)
+            _timed_track(warm, r0[:warm.n], v0[:warm.n], 50, sort_every)
+            ms = _timed_track(tr, r0, v0, wl.nsteps, sort_every)
             res[form] = {"particle_steps_per_s": wl.n * wl.nsteps / (ms / 1e3), "ms": ms}
             hist[form] = tr.r_hist
             del tr, warm
@@ -132,10 +143,10 @@ def run_pusher_sweep(args, dev):
             "workload": "radial_e_solenoid_electrons", "particles": wl.n, "steps": wl.nsteps, "dt": wl.dt,
             "map": "129^3 over a 20 cm cube: E radial 1 MV/m at r = 0.1 m, Bz = 0.5 T cos(pi z / 0.2 m)",
             "error_metric": "per particle max over the start and end records of |r - r64| / max(|r64|, 0.1 m)",
-            "sort_every": args.sort_every, "results": out}
+            "sort_every": sort_every, "results": out}
 
 
-def run_sector_ring(args, dev):
+def run_sector_ring(dev, n=100_000_000, nsteps=50_000, sort_every=100):
     """1e8 protons (5 MeV +-0.5 %) circulating in a four-sector Bz map
     (512^3 float32 over a 1 m cube, 1 T (1 + 0.1 cos 4 theta) - 0.05 T/m r),
     dt = 1e-10 s, 5e4 steps, cell re-sort every 100 steps.  Mixed form over
@@ -146,7 +157,7 @@ def run_sector_ring(args, dev):
     from pypatools_b200 import workloads, Field
     from pypatools_b200.device_fields import DeviceFields
     from pypatools_b200.pusher import DeviceTracker
-    wl = workloads.sector_ring_protons(n=args.n, nsteps=args.nsteps)
+    wl = workloads.sector_ring_protons(n=n, nsteps=nsteps)
     g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
     bf = Field.from_arrays(g, wl.b_values)
     r0, v0 = torch.from_numpy(wl.r0).to(dev), torch.from_numpy(wl.v0).to(dev)
@@ -155,9 +166,9 @@ def run_sector_ring(args, dev):
     out = {}
     dfm = DeviceFields(None, bf, "mixed", dev)
     warm = DeviceTracker("boris", qm, dfm, min(wl.n, 4096), 50, wl.dt, 50, "mixed", device=dev)
-    _timed_track(warm, r0[:warm.n], v0[:warm.n], 50, args.sort_every)
+    _timed_track(warm, r0[:warm.n], v0[:warm.n], 50, sort_every)
     tr = DeviceTracker("boris", qm, dfm, wl.n, wl.nsteps, wl.dt, wl.rec_every, "mixed", device=dev)
-    ms = _timed_track(tr, r0, v0, wl.nsteps, args.sort_every)
+    ms = _timed_track(tr, r0, v0, wl.nsteps, sort_every)
     out["mixed"] = {"particle_steps_per_s": wl.n * wl.nsteps / (ms / 1e3), "ms_job": ms}
     r_mixed_sub = tr.r_hist[:, :sub].clone()
     del tr
@@ -165,12 +176,12 @@ def run_sector_ring(args, dev):
     df64 = DeviceFields(None, bf, "fp64", dev)
     window = max(1, wl.nsteps // 10)
     tr = DeviceTracker("boris", qm, df64, wl.n, window, wl.dt, window, "fp64", device=dev)
-    ms64 = _timed_track(tr, r0, v0, window, args.sort_every)
+    ms64 = _timed_track(tr, r0, v0, window, sort_every)
     out["fp64"] = {"particle_steps_per_s": wl.n * window / (ms64 / 1e3), "ms": ms64, "steps_timed": window}
     del tr
     torch.cuda.empty_cache()
     tr = DeviceTracker("boris", qm, df64, sub, wl.nsteps, wl.dt, wl.rec_every, "fp64", device=dev)
-    _timed_track(tr, r0[:sub].contiguous(), v0[:sub].contiguous(), wl.nsteps, args.sort_every)
+    _timed_track(tr, r0[:sub].contiguous(), v0[:sub].contiguous(), wl.nsteps, sort_every)
     out["mixed_over_fp64"] = out["mixed"]["particle_steps_per_s"] / out["fp64"]["particle_steps_per_s"]
     out["error_vs_fp64"] = _rel_err(r_mixed_sub, tr.r_hist, 0.5)
     out["error_vs_fp64"]["sample"] = f"first {sub} particles, whole job"
@@ -185,7 +196,7 @@ def run_sector_ring(args, dev):
     return {"metric": "particle-steps/s, mixed vs float64, and the mixed form's error (large-scale sector ring)",
             "workload": "sector_ring_protons", "particles": wl.n, "steps": wl.nsteps, "dt": wl.dt,
             "map": "512^3 float32 Bz over a 1 m cube (Bx = By = 0: the Bz-only record layout)",
-            "sort_every": args.sort_every, "map_bytes_mixed": dfm.map_bytes,
+            "sort_every": sort_every, "map_bytes_mixed": dfm.map_bytes,
             "error_metric": "per particle max over the start and end records of |r - r64| / max(|r64|, 0.5 m)",
             "results": out}
 
@@ -475,6 +486,26 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def d2h_bandwidth(dev, gib=2, reps=3):
+    """Device -> pinned host copy rate (GB/s), best of ``reps`` copies of
+    ``gib`` GiB: the link the e2e histories cross."""
+    import torch
+    n = gib << 30
+    d = torch.empty(n, dtype=torch.uint8, device=dev)
+    h = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    best = None
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        h.copy_(d, non_blocking=True)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        best = ms if best is None or ms < best else best
+    del d, h
+    return n / (best / 1e3) / 1e9
+
+
 def max_over_ranks(value, world, device):
     """The slowest rank's device time: replicas report the job as done when
     the last one is (the only collective on the bench path)."""
@@ -487,11 +518,34 @@ def max_over_ranks(value, world, device):
     return float(t.item())
 
 
-def run_reference_arm(args, rank):
+HEADLINE_METRIC = "particle-steps/s, mixed-precision fused Boris + trilinear E/B (RF gap, 1e7 protons, 256^3 map)"
+
+
+def headline_config(n, nsteps, world):
+    """The ``config`` object of the RF-gap line, the same for both arms."""
+    from pypatools_b200 import workloads
+    wl = workloads.rf_gap_protons(n=1, nsteps=nsteps)
+    nodes = wl.grid[0].shape[0]
+    stored = [v for vals in (wl.e_values, wl.b_values) for v in vals.values() if np.any(v)]
+    map_mb = nodes ** 3 * len(stored) * 4 / 1e6            # the {Ez, Bz} record layout: 2 x 4 B per node
+    n_rec = nsteps // wl.rec_every + 1
+    return {"workload": "rf_gap_protons", "particles_per_gpu": n, "steps_per_job": nsteps, "dt": wl.dt,
+            "map": f"{nodes}^3 float32 over a 20 cm cube, stored as {{Ez, Bz}} records ({map_mb:.0f} MB)",
+            "rf_hz": wl.rf_frequency, "snapshot_every": wl.rec_every, "algorithm": "boris", "precision": "mixed",
+            "parallelism": f"replicas x{world}",
+            "l2": (f"inputs larger than L2 (map {map_mb:.0f} MB, mixed state {n * 60 / 1e6:.0f} MB, "
+                   f"snapshots {2 * n_rec * n * 24 / 1e9:.1f} GB)")}
+
+
+def run_reference_arm(args, rank, world):
+    """The reference's CPU path (the C port of it: the reference is Python
+    and its source does not travel) on the host cores, rank 0 only, with
+    the GPU arm's metric and config."""
     if rank != 0:
         return
     from oracle import cpu_baseline
-    res = cpu_baseline.run_reference_arm(args.n, args.nsteps, args.steps, args.warmup)
+    res = cpu_baseline.run_reference_arm(HEADLINE_METRIC, headline_config(args.n, args.nsteps, world),
+                                         args.steps, args.warmup)
     print(json.dumps(res), flush=True)
 
 
@@ -501,7 +555,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        run_reference_arm(args, rank)
+        run_reference_arm(args, rank, world)
         return
 
     import torch
@@ -515,7 +569,7 @@ def main():
     if args.workload != "rf_gap":
         if rank == 0:
             fn = run_pusher_sweep if args.workload == "pusher_sweep" else run_sector_ring
-            print(json.dumps(fn(args, dev)), flush=True)
+            print(json.dumps(fn(dev, args.n, args.nsteps, args.sort_every)), flush=True)
         return
     if world > 1:
         from datetime import timedelta
@@ -628,31 +682,51 @@ def main():
     m = results["mixed"]
     value = total_ps / (m["ms_total"] / 1e3)
 
-    # roofline of the dominant kernel (mixed track kernel): algorithmic bytes
-    # = in-map gathers x 8 corners x stored components x 4 B + state in/out
-    # per launch + snapshot rows written.
+    # Roofline of the dominant kernel (the mixed track kernel), in the terms
+    # this path's measurement plan defines: algorithmic bytes = in-map
+    # gathers x 8 corners x stored components x 4 B + state in/out per
+    # launch + snapshot rows written, against the measured HBM copy
+    # bandwidth.  The gathers of a cell-sorted bunch are served from L1, so
+    # that fraction is a basis, not the kernel's limit: the limit is
+    # instruction issue (the "limiter" object below).
     peak, peak_kind = measured_peaks()
     hits = m["counters"]["map_hits"]
+    psteps = m["counters"]["particle_steps"]
     n_launch = len(m["launch_ms"])
     gather_b = hits * 8 * m["n_comp"] * 4
     state_b = n_launch * n * 2 * 48
     snap_b = args.steps * (wl.nsteps // wl.rec_every + 1) * n * 48
     alg_bytes_per_launch = (gather_b + state_b + snap_b) / max(n_launch, 1)
-    avg_launch_s = float(np.mean(m["launch_ms"])) / 1e3
+    kernel_s = float(np.sum(m["launch_ms"])) / 1e3
+    avg_launch_s = kernel_s / max(n_launch, 1)
     achieved = alg_bytes_per_launch / avg_launch_s / 1e9
+    clk_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    # warp-instructions issued per warp-step in the map and in field-free
+    # drift, from the ncu instruction counts of the kernel as built
+    # (profiles/track_mixed_kernel_rf_gap_1e6_*.txt)
+    inst = (hits * WARP_INST_PER_WARP_STEP["map"] + (psteps - hits) * WARP_INST_PER_WARP_STEP["drift"]) / 32.0
+    issue_peak = n_sm * 4 * clk_hz                  # one warp-instruction per scheduler per clock
+    l1_peak = n_sm * 128 * clk_hz / 1e9             # 128 B per SM per clock
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "basis": "algorithmic bytes (in-map corner gathers of the stored components + state + snapshot "
+                         "rows) at the measured HBM copy bandwidth; the gathers are L1-served, so this is not "
+                         "the kernel's limit (see limiter)",
                 "traffic": MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH * n,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one in-map 100-step launch "
                                   "at 1e6 protons (profiles/track_mixed_kernel_rf_gap_1e6_in_map.txt), scaled "
-                                  "by particle count; the gathers are served from L1/L2",
+                                  "by particle count",
                 "peak_kind": f"{peak_kind} hbm_gbs",
                 "kernel": "track_mixed_kernel<BORIS,RF,Ez|Bz layout>", "avg_launch_ms": avg_launch_s * 1e3,
-                "in_map_fraction": hits / max(1, m["counters"]["particle_steps"]),
-                "note": "algorithmic bytes as defined for this path count every corner gather of the "
-                        "stored components, but the gathers of cell-sorted particles are served from L1 "
-                        "and the DRAM traffic is the state in and out (traffic); the kernel is not "
-                        "HBM-bound: ncu shows it issue-bound in the map (86 % issue-active, 205 "
-                        "warp-instructions per warp-step)"}
+                "in_map_fraction": hits / max(1, psteps),
+                "limiter": {"kind": "instruction issue",
+                            "issue_frac": inst / (issue_peak * kernel_s),
+                            "warp_inst_per_s": inst / kernel_s, "peak_warp_inst_per_s": issue_peak,
+                            "warp_inst_per_warp_step": dict(WARP_INST_PER_WARP_STEP),
+                            "l1_gather_gbs": gather_b / kernel_s / 1e9, "l1_peak_gbs": l1_peak,
+                            "l1_frac": gather_b / kernel_s / 1e9 / l1_peak,
+                            "model": f"({n_sm} SMs x 4 schedulers x median SM clock) for issue; {n_sm} SMs x "
+                                     "128 B/clock for L1; instruction counts per warp-step from ncu"}}
 
     # e2e through the public API with host buffers (H2D of r0/v0/phase, D2H of the histories)
     e2e = None
@@ -672,45 +746,62 @@ def main():
         n_rec = wl.nsteps // wl.rec_every + 1
         # per step: r0 and v0 (n,3) float64 plus the n RF phases in; both
         # (n_rec, n, 3) float64 histories out
+        d2h_bytes = 2 * n_rec * n * 24
+        d2h_gbs = d2h_bandwidth(dev)
+        # the bound this path can reach: the device job, then the histories at the
+        # link's measured rate (the copies of early records overlap the job)
+        bound = n * wl.nsteps / (m["ms_per_job"] / 1e3 + d2h_bytes / (d2h_gbs * 1e9))
         e2e = {"value": n * wl.nsteps * args.e2e_steps * world / dt_e2e, "unit": "particle-steps/s",
                "h2d_bytes_per_step": int(2 * n * 24 + n * 8),
-               "d2h_bytes_per_step": int(2 * n_rec * n * 24),
-               "api": "PusherGPU.track_batch (numpy in, numpy histories out)", "steps": args.e2e_steps}
+               "d2h_bytes_per_step": int(d2h_bytes),
+               "api": "PusherGPU.track_batch (numpy in, numpy histories out)", "steps": args.e2e_steps,
+               "s_per_call": dt_e2e / args.e2e_steps, "d2h_gbs_measured": d2h_gbs,
+               "bound_device_plus_d2h": bound, "frac_of_bound": n * wl.nsteps / (dt_e2e / args.e2e_steps) / bound}
         del rh, vh
 
-    deposit = electrodes = loader = space_charge = None
-    if rank == 0:
+    deposit = electrodes = loader = space_charge = sweep = ring = None
+    if rank == 0 and not args.no_legs:
         deposit = run_deposit(d_r0, dev)
         space_charge = run_space_charge(d_r0, dev)
         electrodes = run_electrodes(dev)
         loader = run_loaders(dev)
+    del d_r0, d_v0, d_phase
+    torch.cuda.empty_cache()
+    if rank == 0 and not args.no_sweep:
+        sweep = run_pusher_sweep(dev)
+        torch.cuda.empty_cache()
+    if rank == 0 and not args.no_sector_ring:
+        ring = run_sector_ring(dev)
+        torch.cuda.empty_cache()
 
     serving = None
-    if args.serve_jobs > 0:
-        torch.cuda.empty_cache()
+    if rank == 0 and args.serve_jobs > 0:
         serving = run_serving(args.serve_jobs, dev)
 
     cpu = None
     if rank == 0:
         from oracle import cpu_baseline
-        cpu = cpu_baseline.sample(n_sample=20_000, steps=20, in_map_fraction=roofline["in_map_fraction"])
+        cpu = cpu_baseline.sample(n_sample=20_000, steps=20)
+        cpu["in_map_fraction_gpu_counters"] = roofline["in_map_fraction"]
 
     if rank == 0:
         f64 = results.get("fp64")
+        ratio = (f64["ms_total"] / m["ms_total"]) if f64 else None
+        targets = {"mixed_over_fp64": ratio, "mixed_over_fp64_target": 5.0,
+                   "speed_target_met": (ratio >= 5.0) if ratio is not None else None,
+                   "max_rel_pos": err["max_rel_pos"] if err else None, "max_rel_pos_target": 1e-6,
+                   "error_target_met": (err["max_rel_pos"] <= 1e-6) if err else None}
         line = {
-            "metric": "particle-steps/s, mixed-precision fused Boris + trilinear E/B (RF gap, 1e7 protons, 256^3 map)",
+            "metric": HEADLINE_METRIC,
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": m["ms_per_job"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 time/phase, float-float velocity)",
             "data": "synthetic (seeded pypatools_b200.workloads.rf_gap_protons)",
-            "config": {"workload": "rf_gap_protons", "particles_per_gpu": n, "steps_per_job": wl.nsteps,
-                       "dt": wl.dt, "map": "256^3 float32 E+B over a 20 cm cube", "rf_hz": wl.rf_frequency,
-                       "snapshot_every": wl.rec_every, "algorithm": "boris", "precision": "mixed",
-                       "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (map 537 MB, state 480 MB, snapshots 19.7 GB)"},
+            "config": headline_config(n, wl.nsteps, world),
             "fp64": ({"value": total_ps / (f64["ms_total"] / 1e3), "ms_per_step": f64["ms_per_job"],
                       "launches": f64["launches"]} if f64 else None),
-            "mixed_over_fp64": (f64["ms_total"] / m["ms_total"]) if f64 else None,
+            "mixed_over_fp64": ratio,
+            "targets": targets,
             "phases": phases,
             "error_vs_fp64": err,
             "roofline": roofline,
@@ -718,6 +809,8 @@ def main():
             "e2e": e2e,
             "gpu_launches": m["launches"],
             "clocks": clocks,
+            "pusher_sweep": sweep,
+            "sector_ring": ring,
             "serving": serving,
             "deposit": deposit,
             "electrodes": electrodes,

@@ -46,7 +46,7 @@
 extern "C" {
 #endif
 
-#define PPT_ABI_VERSION 2
+#define PPT_ABI_VERSION 3
 
 /* status codes */
 #define PPT_OK               0
@@ -172,10 +172,11 @@ int ppt_field_eval(const ppt_fields* fields, int64_t n, const double* pts,
 /* Particle state on the device, structure of arrays:
  *   PPT_PREC_F64:   f64[6*n]  = x | y | z | w_x | w_y | w_z
  *   PPT_PREC_MIXED: i32[3*n]  = cell i | j | k  (on map 0's grid)
- *                   f32[9*n]  = offset x|y|z | w_hi x|y|z | w_lo x|y|z
- *                   (position = lo + (cell + offset) d; the offset is in [0, 1]
- *                   after steps that may see a field and may pass 1 between
- *                   the whole-cell carries of field-free steps)
+ *                   f32[12*n] = offset_hi x|y|z | w_hi x|y|z | w_lo x|y|z | offset_lo x|y|z
+ *                   (position = lo + (cell + offset_hi + offset_lo) d; the high
+ *                   offset is in [0, 1] after steps that may see a field and
+ *                   may pass 1 between the whole-cell carries of field-free
+ *                   steps)
  * w is the velocity v [m/s], or u = gamma v for BORIS_REL / VAY. */
 typedef struct {
     int32_t precision;
@@ -215,6 +216,11 @@ typedef struct {
     unsigned long long* counters; /* device u64[2]: +in-map gathers, +particle steps; or NULL */
     const struct ppt_surface* surface; /* electrode surface (float64 form), or NULL: see below */
     uint8_t* active;      /* with a surface: device uint8[n] in ROW order, 1 = still tracked */
+    const double* dt_rows; /* device float64[n] in ROW order: one time step per particle for the
+                            * float64 form's RK4 and rk4_rel (the reference's batch RK4 step
+                            * broadcasts an array dt over the particles, pusher.py:815-816);
+                            * NULL = dt for every particle.  Other algorithms and the mixed form:
+                            * PPT_ERR_UNSUPPORTED. */
 } ppt_track_args;
 
 /* Advance every particle nsteps steps in ONE kernel launch, state kept in
@@ -396,8 +402,10 @@ int ppt_moments(int64_t n, const double* r, const double* v, double mass_mev,
  * device, are not allowed).  No counterpart in the reference.
  * Scratch: a static 52 KB device array, held by every GPU that loads the
  * library until the process exits.  The first call on a device looks up its
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race.
+ * address (cudaGetSymbolAddress), and so does the first call in a new context
+ * of that device (after cudaDeviceReset, or in a context the caller made
+ * current); make that first call before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race.
  * n must be in [1, 2^53]; anything else returns PPT_ERR_ARG. */
 int ppt_moments_noalloc(int64_t n, const double* r, const double* v, double mass_mev,
                         double* out, void* stream);

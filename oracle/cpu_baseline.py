@@ -88,29 +88,67 @@ def _time_window(wl, omap, r0, v0, phase, steps):
     return time.perf_counter() - t
 
 
-def sample(n_sample=20_000, steps=20, in_map_fraction=None):
+# RF-gap job: 2e4 steps; every proton has left the 20 cm map within its
+# first ~1300 steps (it enters at z in +-6.9 cm at 1.4e7 m/s).
+RF_GAP_STEPS = 20_000
+
+
+def in_map_fraction(n_sample=2000, window=1600, job_steps=RF_GAP_STEPS):
+    """Share of the RF-gap job's particle-steps whose field evaluation falls
+    inside the map, from the oracle's own tracks: the steps of a bunch sample
+    whose start position lies in the map's node box, over the first
+    ``window`` steps (the sample must have left the map by then: checked),
+    divided by the job's particle-steps."""
+    from pypatools_b200 import workloads
+    wl = workloads.rf_gap_protons(n=n_sample, nsteps=window)
+    omap, keep = make_map(wl.grid, wl.e_values, wl.b_values)
+    rh, _ = track("boris", wl.r0, wl.v0, omap, window, wl.dt, wl.species.q_over_m, rec=1,
+                  omega=2 * np.pi * wl.rf_frequency, phase=wl.rf_phase)
+    lo = np.array([g[0] for g in wl.grid])
+    hi = np.array([g[-1] for g in wl.grid])
+    inside = np.all((rh >= lo) & (rh <= hi), axis=2)          # (window + 1, n)
+    if inside[-1].any():
+        raise RuntimeError("in_map_fraction: particles still in the map after the window")
+    del keep
+    return float(inside[:-1].sum()) / (n_sample * job_steps)
+
+
+def blended_sample(n_sample=20_000, steps=20, fraction=None):
     """Boris on the RF-gap workload: a window of ``steps`` steps of
     ``n_sample`` particles in the map (the bunch's start) and the same window
-    after the bunch has left it (the drift phase that makes up most of the
-    job); rates combined by the job's in-map fraction when given."""
+    after the bunch has left it (the drift that makes up most of the job),
+    combined by the job's in-map fraction (``in_map_fraction()`` unless
+    given): seconds per ``n_sample x steps`` particle-steps of the job's mix,
+    and the two phase rates."""
     from pypatools_b200 import workloads
     wl = workloads.rf_gap_protons(n=n_sample, nsteps=steps)
     omap, keep = make_map(wl.grid, wl.e_values, wl.b_values)
     load()
+    f = in_map_fraction() if fraction is None else float(fraction)
     _time_window(wl, omap, wl.r0[:64], wl.v0[:64], wl.rf_phase[:64], 2)     # warm caches / threads
     t_in = _time_window(wl, omap, wl.r0, wl.v0, wl.rf_phase, steps)
     r_out = wl.r0.copy()
     r_out[:, 2] += 0.35                                                     # past the 20 cm map
     t_out = _time_window(wl, omap, r_out, wl.v0, wl.rf_phase, steps)
-    ps = n_sample * steps
-    rate_in, rate_out = ps / t_in, ps / t_out
-    f = in_map_fraction
-    value = rate_in if f is None else 1.0 / (f / rate_in + (1.0 - f) / rate_out)
     del keep
-    return {"value": value, "unit": "particle-steps/s", "cores": int(load().oracle_threads()), "kind": "port",
-            "sample": (f"boris, {n_sample} particles x {steps} steps in the map and x {steps} steps past it "
-                       f"(RF gap workload, float64); combined by the job's in-map fraction"),
-            "rate_in_map": rate_in, "rate_drift": rate_out,
+    ps = n_sample * steps
+    return {"seconds": f * t_in + (1.0 - f) * t_out, "particle_steps": ps, "fraction": f,
+            "rate_in_map": ps / t_in, "rate_drift": ps / t_out}
+
+
+def _describe(n_sample, steps, f):
+    return (f"boris, float64, RF gap workload: {n_sample} particles x {steps} steps in the map and x {steps} "
+            f"steps past it, combined by the job's in-map fraction {f:.4f} (from the oracle's own tracks)")
+
+
+def sample(n_sample=20_000, steps=20, in_map_fraction=None):
+    """The bench line's cpu_baseline object: the job-mix rate of
+    ``blended_sample``."""
+    b = blended_sample(n_sample, steps, in_map_fraction)
+    return {"value": b["particle_steps"] / b["seconds"], "unit": "particle-steps/s",
+            "cores": int(load().oracle_threads()), "kind": "port",
+            "sample": _describe(n_sample, steps, b["fraction"]),
+            "in_map_fraction": b["fraction"], "rate_in_map": b["rate_in_map"], "rate_drift": b["rate_drift"],
             "cpu": _cpu_model()}
 
 
@@ -124,30 +162,29 @@ def _cpu_model():
     return "unknown"
 
 
-def run_reference_arm(n, nsteps, steps, warmup):
+def run_reference_arm(metric, config, steps, warmup):
     """bench.py --impl reference: the CPU port of the reference algorithm on
-    all host threads, each step a bounded sample of the RF-gap job."""
-    from pypatools_b200 import workloads
+    all host threads.  Each bench step is a bounded sample of the RF-gap job
+    with the job's phase mix (``blended_sample``); ``metric`` and ``config``
+    are the GPU arm's, so the two lines describe the same workload."""
     n_sample, window = 20_000, 20
-    wl = workloads.rf_gap_protons(n=n_sample, nsteps=window)
-    omap, keep = make_map(wl.grid, wl.e_values, wl.b_values)
+    f = in_map_fraction()
     for _ in range(max(1, warmup)):
-        _time_window(wl, omap, wl.r0, wl.v0, wl.rf_phase, 2)
-    times = [_time_window(wl, omap, wl.r0, wl.v0, wl.rf_phase, window) for _ in range(steps)]
-    total = sum(times)
+        blended_sample(2000, 2, f)
+    runs = [blended_sample(n_sample, window, f) for _ in range(steps)]
+    total = sum(r["seconds"] for r in runs)
     value = n_sample * window * steps / total
-    del keep
-    res = {"impl": "reference", "metric": "particle-steps/s, mixed-precision fused Boris + trilinear E/B "
-                                          "(RF gap, 1e7 protons, 256^3 map)",
+    cores = int(load().oracle_threads())
+    res = {"impl": "reference", "metric": metric,
            "value": value, "unit": "particle-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
            "steps": steps, "warmup": warmup, "ms_per_step": 1e3 * total / steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded pypatools_b200.workloads.rf_gap_protons)",
-           "config": {"workload": "rf_gap_protons", "particles_per_gpu": n, "steps_per_job": nsteps,
-                      "sample": f"{n_sample} particles x {window} steps per bench step (in-map phase)"},
-           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": int(load().oracle_threads()),
-                            "kind": "port", "sample": f"boris, {n_sample} particles x {window} steps, float64",
-                            "cpu": _cpu_model()},
+           "config": config,
+           "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+                            "sample": _describe(n_sample, window, f), "in_map_fraction": f,
+                            "rate_in_map": sum(r["rate_in_map"] for r in runs) / steps,
+                            "rate_drift": sum(r["rate_drift"] for r in runs) / steps, "cpu": _cpu_model()},
            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return res
 

@@ -353,24 +353,29 @@ class _Fields:
 
 
 def rk4_step(r, v, fields, t, dt, qm, rel):
-    """pusher.py:803-892 with stage field times t, t+dt/2, t+dt/2, t+dt."""
+    """pusher.py:803-892 with stage field times t, t+dt/2, t+dt/2, t+dt.
+    ``dt`` may hold one value per particle: the reference broadcasts such an
+    array over each particle's three components (pusher.py:815-816)."""
     deriv = rk4_rel_deriv if rel else lorentz_accel
+    ts = dt
+    if np.ndim(dt) == 1:
+        dt = np.asarray(dt, dtype=np.float64)[:, None]
     e1, b1 = fields(r, t)
     k1_v = deriv(v, e1, b1, qm)
     k1_r = v.copy()
     r2 = r + 0.5 * dt * k1_r
     v2 = v + 0.5 * dt * k1_v
-    e2, b2 = fields(r2, t + 0.5 * dt)
+    e2, b2 = fields(r2, t + 0.5 * ts)
     k2_v = deriv(v2, e2, b2, qm)
     k2_r = v2.copy()
     r3 = r + 0.5 * dt * k2_r
     v3 = v + 0.5 * dt * k2_v
-    e3, b3 = fields(r3, t + 0.5 * dt)
+    e3, b3 = fields(r3, t + 0.5 * ts)
     k3_v = deriv(v3, e3, b3, qm)
     k3_r = v3.copy()
     r4 = r + dt * k3_r
     v4 = v + dt * k3_v
-    e4, b4 = fields(r4, t + dt)
+    e4, b4 = fields(r4, t + ts)
     k4_v = deriv(v4, e4, b4, qm)
     k4_r = v4.copy()
     r_new = r + (dt / 6.0) * (k1_r + 2.0 * k2_r + 2.0 * k3_r + k4_r)

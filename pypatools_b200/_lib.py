@@ -16,6 +16,7 @@ ERRORS = {-1: "PPT_ERR_ARG", -2: "PPT_ERR_OOM", -3: "PPT_ERR_CUDA", -4: "PPT_ERR
 
 ALG_IDS = {"leapfrog": 0, "boris": 1, "rk4": 2, "yoshida": 3, "vay_rel": 4, "rk4_rel": 5,
            "yoshida_rel": 6, "boris_rel": 7, "vay": 8}
+ABI_VERSION = 3
 PREC_F64, PREC_MIXED = 0, 1
 DTYPE_F64, DTYPE_F32 = 0, 1
 TRACK_INIT, TRACK_FINAL = 1, 2
@@ -56,7 +57,8 @@ class TrackArgs(ctypes.Structure):
                 ("dt", c_double), ("q_over_m", c_double), ("t0", c_double),
                 ("rf_omega", c_double), ("rf_phase", c_void_p), ("r_hist", c_void_p),
                 ("v_hist", c_void_p), ("order", c_void_p), ("status", c_void_p),
-                ("counters", c_void_p), ("surface", c_void_p), ("active", c_void_p)]
+                ("counters", c_void_p), ("surface", c_void_p), ("active", c_void_p),
+                ("dt_rows", c_void_p)]
 
 
 class JobDesc(ctypes.Structure):
@@ -131,7 +133,7 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.ppt_abi_version() != 2:
+    if lib.ppt_abi_version() != ABI_VERSION:
         raise ImportError("libppt.so ABI version mismatch; rebuild it")
     _lib = lib
     return lib

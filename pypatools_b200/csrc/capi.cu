@@ -85,8 +85,19 @@ extern "C" int ppt_track(ppt_state* st, const ppt_fields* fields, const ppt_trac
             P.surf = a->surface->dev;
             P.active = a->active;
         }
+        if (a->dt_rows) {
+            // the reference's batch RK4 step is the one that broadcasts an array dt
+            // (pusher.py:815-816); its other pushers take a float
+            if (st->algorithm != PPT_ALG_RK4 && st->algorithm != PPT_ALG_RK4_REL)
+                return fail(PPT_ERR_UNSUPPORTED, "a per-particle dt needs the rk4 or rk4_rel algorithm");
+            P.dt_rows = a->dt_rows;
+        }
+        // the launch's per-step RF table covers steps step0 .. step0 + nsteps
+        // (the closing half step reads the last one); a per-particle dt has none
+        P.rf_tab_n = (rf && !a->dt_rows && a->nsteps + 1 <= 512) ? (int32_t)(a->nsteps + 1) : 0;
         return launch_track_f64(P, st->algorithm, rf, a->surface != nullptr, s);
     }
+    if (a->dt_rows) return fail(PPT_ERR_UNSUPPORTED, "a per-particle dt runs in the float64 form");
     if (a->surface && st->algorithm != PPT_ALG_BORIS)
         return fail(PPT_ERR_UNSUPPORTED, "electrode surfaces run in the float64 form and the mixed form's boris");
     if (a->surface && !a->active) return fail(PPT_ERR_ARG, "a surface needs the active array");

@@ -177,6 +177,8 @@ extern "C" int ppt_moments(int64_t n, const double* r, const double* v, double m
 // ---------------------------------------------------------------------------
 #include <mutex>
 
+#include <cudaTypedefs.h>   // CUcontext and the cuCtxGetCurrent signature (called through the runtime)
+
 namespace ppt {
 
 // 11 partial sums for each of up to kMomBlocks blocks, then 16 means.
@@ -186,19 +188,51 @@ static __device__ __align__(256) double g_moments_scratch[kNoAllocScratchDoubles
 constexpr int kMaxDevices = 64;
 static std::mutex g_scratch_mutex;
 static double* g_scratch_addr[kMaxDevices] = {};
+static CUcontext g_scratch_ctx[kMaxDevices] = {};
 
-// Device address of g_moments_scratch on the current device, looked up once
-// per device (host code only has a host-side stand-in for the symbol).
+// The calling thread's current context (the runtime's entry-point query
+// gives the driver function without linking the driver library).
+static int current_context(CUcontext* ctx) {
+    static PFN_cuCtxGetCurrent_v4000 get = nullptr;
+    if (!get) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetDriverEntryPoint(cuCtxGetCurrent)");
+        if (q != cudaDriverEntryPointSuccess || !fn) return fail(PPT_ERR_CUDA, "cuCtxGetCurrent is not available");
+        get = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
+    }
+    if (get(ctx) != CUDA_SUCCESS) return fail(PPT_ERR_CUDA, "cuCtxGetCurrent failed");
+    return PPT_OK;
+}
+
+// Device address of g_moments_scratch in the current device's context,
+// looked up once per device and context (host code only has a host-side
+// stand-in for the symbol).  The module, and with it the array, is loaded
+// anew in a new context -- after cudaDeviceReset, or in a context the caller
+// made current itself -- so the address is looked up again when the context
+// differs from the one it was taken in.
 static int noalloc_scratch(double** out) {
     int dev = 0;
     PPT_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) return fail(PPT_ERR_UNSUPPORTED, "device ordinal above 63");
+    CUcontext ctx = nullptr;
+    int rc = current_context(&ctx);
+    if (rc) return rc;
+    if (!ctx) {
+        // no context current on this thread yet: the device's primary context
+        // (cudaSetDevice initialises and binds it; it allocates nothing)
+        PPT_CUDA_TRY(cudaSetDevice(dev));
+        rc = current_context(&ctx);
+        if (rc) return rc;
+    }
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_addr[dev]) {
+    if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_moments_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(moments scratch)");
         g_scratch_addr[dev] = static_cast<double*>(p);
+        g_scratch_ctx[dev] = ctx;
     }
     *out = g_scratch_addr[dev];
     return PPT_OK;

@@ -76,6 +76,24 @@ __host__ __device__ constexpr int layout_width(int layout) {
 __host__ __device__ constexpr bool layout_has_e(int layout) { return (layout & 0x07) != 0; }
 __host__ __device__ constexpr bool layout_has_b(int layout) { return (layout & 0x38) != 0; }
 
+// Components a record layout can make non-zero: bit a of e_bits (b_bits)
+// is E_a (B_a); the six-component layout also carries the constant parts.
+// x * 0 and x + 0 are not identities in IEEE arithmetic (NaN, signed
+// zeros), so the compiler keeps every operation on a component that is
+// zero by construction unless the code leaves it out: the Boris kernels of
+// both precision forms do, at compile time, from these masks.
+__host__ __device__ constexpr int e_bits(int L) { return L & 7; }
+__host__ __device__ constexpr int b_bits(int L) { return (L >> 3) & 7; }
+__host__ __device__ constexpr bool bit(int m, int a) { return ((m >> a) & 1) != 0; }
+// components of p x q that can be non-zero when q has the components of qm
+__host__ __device__ constexpr int cross_bits(int qm) {
+    return ((bit(qm, 1) || bit(qm, 2)) ? 1 : 0) | ((bit(qm, 2) || bit(qm, 0)) ? 2 : 0) |
+           ((bit(qm, 0) || bit(qm, 1)) ? 4 : 0);
+}
+// velocity components a Boris step can change under layout L
+__host__ __device__ constexpr int boris_bits(int L) { return e_bits(L) | cross_bits(b_bits(L)); }
+
+
 struct MapDev {
     const void* data;
     int64_t sx;       // node stride of i  (= ny*nz)
@@ -230,6 +248,24 @@ __device__ __forceinline__ V3 gather_f64(const MapDev& m, const Cell& c, int off
         ldg_f64x4(base + node * S + off, v[q][0], v[q][1], v[q][2], v[q][3]);
     }
     // corner q = di*4 + dj*2 + dk
+    V3 o;
+    o.x = tri(v[0][0], v[4][0], v[2][0], v[6][0], v[1][0], v[5][0], v[3][0], v[7][0], c.tx, c.ty, c.tz);
+    o.y = tri(v[0][1], v[4][1], v[2][1], v[6][1], v[1][1], v[5][1], v[3][1], v[7][1], c.tx, c.ty, c.tz);
+    o.z = tri(v[0][2], v[4][2], v[2][2], v[6][2], v[1][2], v[5][2], v[3][2], v[7][2], c.tx, c.ty, c.tz);
+    return o;
+}
+
+// gather_f64 for a record stride S known at compile time.
+template <int S>
+__device__ __forceinline__ V3 gather_f64s(const MapDev& m, const Cell& c, int off) {
+    const double* base = static_cast<const double*>(m.data);
+    double v[8][4];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int di = (q >> 2) & 1, dj = (q >> 1) & 1, dk = q & 1;
+        const int64_t node = c.base + di * m.sx + dj * m.sy + dk;
+        ldg_f64x4(base + node * S + off, v[q][0], v[q][1], v[q][2], v[q][3]);
+    }
     V3 o;
     o.x = tri(v[0][0], v[4][0], v[2][0], v[6][0], v[1][0], v[5][0], v[3][0], v[7][0], c.tx, c.ty, c.tz);
     o.y = tri(v[0][1], v[4][1], v[2][1], v[6][1], v[1][1], v[5][1], v[3][1], v[7][1], c.tx, c.ty, c.tz);

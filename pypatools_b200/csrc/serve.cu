@@ -8,11 +8,16 @@
 // `chunk` steps with one persistent kernel per (form, algorithm, RF, mixed
 // map layout) class --
 // blocks take (job, 128-particle block) items from a device queue -- followed
-// by a one-thread-per-job kernel that advances the step counters.  A tick
-// reads nothing from the host and synchronises nothing, so the host can
-// capture it once per job set in a CUDA graph and replay it; jobs that finish
-// simply find their done flag set on later replays.  No reference counterpart:
-// the reference runs one track_batch call at a time (pusher.py:894-1012).
+// by a one-thread-per-job kernel that advances the step counters.  The class
+// kernels of a tick run concurrently: each is issued on a stream of its own
+// that forks from the caller's stream and joins it again before the counter
+// kernel (event dependencies, which a CUDA-graph capture records as parallel
+// branches), so a class with few items no longer leaves the SMs idle while
+// it drains.  A tick reads nothing from the host and synchronises nothing, so
+// the host can capture it once per job set in a CUDA graph and replay it;
+// jobs that finish simply find their done flag set on later replays.  No
+// reference counterpart: the reference runs one track_batch call at a time
+// (pusher.py:894-1012).
 #include <cstring>
 #include <vector>
 
@@ -30,6 +35,9 @@ struct ppt_jobs {
         ppt::JobQueueDev Q;
     };
     std::vector<Class> classes;
+    std::vector<cudaStream_t> lanes;   // one stream per class (non-blocking), forked from the tick's stream
+    std::vector<cudaEvent_t> joins;    // per lane: its class kernel is done
+    cudaEvent_t fork = nullptr;        // the tick's stream reached the class kernels
     std::vector<char> image;   // host copy of the device table (kept for the upload's lifetime)
     unsigned* d_queues;
     int64_t* d_steps;
@@ -39,9 +47,10 @@ struct ppt_jobs {
 
 namespace ppt {
 
-// classes: (form, algorithm, RF, record layout of a mixed job's map)
-constexpr int kLayouts[] = {kLayFull, kLayE, kLayB, kLayExEyBz, kLayEzBz, kLayBz};
-constexpr int kNumLayouts = 6;
+// classes: (form, algorithm, RF, record layout the job's kernel is
+// specialised on; 0 = a float64 job's run-time dispatch over its maps)
+constexpr int kLayouts[] = {kLayFull, kLayE, kLayB, kLayExEyBz, kLayEzBz, kLayBz, 0};
+constexpr int kNumLayouts = 7;
 constexpr int kMaxClasses = 2 * PPT_ALG_COUNT * 2 * kNumLayouts;
 
 static int layout_index(int layout) {
@@ -173,7 +182,8 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
         }
         reinterpret_cast<int64_t*>(img + L.steps)[j] = jobs[j].steps_done;
         const int rf = jobs[j].rf_phase != nullptr;
-        const int lay = jobs[j].state.precision == PPT_PREC_MIXED ? layout_index(mix[j].map.layout) : 0;
+        const int lay = layout_index(jobs[j].state.precision == PPT_PREC_MIXED ? mix[j].map.layout
+                                                                               : f64_single_layout(f64[j]));
         cls[j] = ((jobs[j].state.precision * PPT_ALG_COUNT + jobs[j].state.algorithm) * 2 + rf) * kNumLayouts + lay;
     }
     int pos = 0, ipos = 0;
@@ -210,13 +220,32 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
         K.Q.chunk = 0;
         H->classes.push_back(K);
     }
+    // one stream per class beyond the first, which runs on the caller's stream
+    H->fork = nullptr;
+    if (H->classes.size() > 1) {
+        cudaError_t e = cudaEventCreateWithFlags(&H->fork, cudaEventDisableTiming);
+        for (size_t i = 1; e == cudaSuccess && i < H->classes.size(); ++i) {
+            cudaStream_t st;
+            cudaEvent_t ev;
+            e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+            if (e != cudaSuccess) break;
+            H->lanes.push_back(st);
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) break;
+            H->joins.push_back(ev);
+        }
+        if (e != cudaSuccess) {
+            ppt_jobs_destroy(H);
+            return cuda_fail(e, "job class streams");
+        }
+    }
     H->d_queues = reinterpret_cast<unsigned*>(dev + L.queues);
     H->d_steps = reinterpret_cast<int64_t*>(dev + L.steps);
     H->d_done = reinterpret_cast<int*>(dev + L.done);
     H->d_total = reinterpret_cast<const int64_t*>(dev + L.total);
     cudaError_t e = cudaMemcpyAsync(scratch, img, L.bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) {
-        delete H;
+        ppt_jobs_destroy(H);
         return cuda_fail(e, "job table upload");
     }
     *out = H;
@@ -229,13 +258,19 @@ extern "C" int ppt_jobs_tick(ppt_jobs* H, int64_t chunk, void* stream) {
     if (H->n_jobs == 0) return PPT_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     PPT_CUDA_TRY(cudaMemsetAsync(H->d_queues, 0, sizeof(unsigned) * kMaxClasses, s));
-    for (auto& K : H->classes) {
+    if (H->fork) PPT_CUDA_TRY(cudaEventRecord(H->fork, s));
+    for (size_t i = 0; i < H->classes.size(); ++i) {
+        const auto& K = H->classes[i];
         JobQueueDev Q = K.Q;
         Q.chunk = chunk;
-        int rc = K.precision == PPT_PREC_F64 ? launch_f64_jobs(Q, K.algorithm, K.rf != 0, K.grid, s)
-                                             : launch_mixed_jobs(Q, K.algorithm, K.layout, K.rf != 0, K.grid, s);
+        cudaStream_t cs = i == 0 ? s : H->lanes[i - 1];
+        if (i > 0) PPT_CUDA_TRY(cudaStreamWaitEvent(cs, H->fork, 0));
+        int rc = K.precision == PPT_PREC_F64 ? launch_f64_jobs(Q, K.algorithm, K.layout, K.rf != 0, K.grid, cs)
+                                             : launch_mixed_jobs(Q, K.algorithm, K.layout, K.rf != 0, K.grid, cs);
         if (rc) return rc;
+        if (i > 0) PPT_CUDA_TRY(cudaEventRecord(H->joins[i - 1], cs));
     }
+    for (size_t i = 1; i < H->classes.size(); ++i) PPT_CUDA_TRY(cudaStreamWaitEvent(s, H->joins[i - 1], 0));
     jobs_advance_kernel<<<(H->n_jobs + 255) / 256, 256, 0, s>>>(H->n_jobs, H->d_steps, H->d_done, H->d_total, chunk);
     PPT_CUDA_TRY(cudaGetLastError());
     return PPT_OK;
@@ -249,6 +284,12 @@ extern "C" int ppt_jobs_progress(const ppt_jobs* H, int64_t** steps, int32_t** d
 }
 
 extern "C" int ppt_jobs_destroy(ppt_jobs* H) {
+    if (!H) return PPT_OK;
+    // work still queued on the lanes completes first: destroying a stream or
+    // an event does not cancel it
+    for (cudaStream_t st : H->lanes) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : H->joins) cudaEventDestroy(ev);
+    if (H->fork) cudaEventDestroy(H->fork);
     delete H;
     return PPT_OK;
 }

@@ -219,7 +219,7 @@ static SortLayout sort_layout(int64_t n) {
     L.tiles = o; o += align256((nb / kScanTile + 2) * 4);
     L.ctrl = o;  o += 256;
     L.tmp64 = o; o += align256((size_t)n * 6 * 8);     // float64 state
-    L.tmp32 = o; o += align256((size_t)n * 12 * 4);    // mixed: 3 int32 + 9 float32 columns
+    L.tmp32 = o; o += align256((size_t)n * 15 * 4);    // mixed: 3 int32 + 12 float32 columns
     L.order = o; o += align256((size_t)n * 8);
     L.phase = o; o += align256((size_t)n * 8);
     L.total = o;
@@ -299,12 +299,12 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
                                                           nullptr, nullptr, order, order_tmp, rf_phase, phase_tmp);
         copy_back(tmp64, st->f64, (size_t)n * 6 * 8, ctrl, n, s);
     } else {
-        // 3 int32 cell columns then 9 float32 columns, all 4-byte words
+        // 3 int32 cell columns then 12 float32 columns, all 4-byte words
         sort_scatter<<<grid_for(n, block), block, 0, s>>>(
-            n, key, count, ctrl, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 9,
+            n, key, count, ctrl, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 12,
             reinterpret_cast<const uint32_t*>(st->f32), tmp32, order, order_tmp, rf_phase, phase_tmp);
         copy_back(tmp32, st->i32, (size_t)n * 3 * 4, ctrl, n, s);
-        copy_back(tmp32 + 3 * n, st->f32, (size_t)n * 9 * 4, ctrl, n, s);
+        copy_back(tmp32 + 3 * n, st->f32, (size_t)n * 12 * 4, ctrl, n, s);
     }
     copy_back(order_tmp, order, (size_t)n * 8, ctrl, n, s);
     if (rf_phase) copy_back(phase_tmp, rf_phase, (size_t)n * 8, ctrl, n, s);

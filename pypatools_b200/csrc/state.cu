@@ -71,13 +71,19 @@ __global__ void load_mixed_kernel(int64_t n, const double* __restrict__ r, const
             u = 0.0;
         }
         int cell = (int)fl;
-        float f = (float)(u - fl);
-        if (f >= 1.0f) {
+        const double off = u - fl;           // in [0, 1)
+        // the high word on the 2^-22 grid the Boris family's steps keep it on
+        // (exact additions, track_mixed.cu add_cells_q), the rest in the low word
+        const double fq = rint(off * 0x1p22) * 0x1p-22;
+        float f = (float)fq;
+        float f_lo = (float)(off - fq);
+        if (f >= 1.0f) {                     // off within 2^-23 of 1: the next cell's node
             f = 0.0f;
             cell += 1;
         }
         ci[c * n + s] = cell;
         fs[c * n + s] = f;
+        fs[(9 + c) * n + s] = f_lo;
         float hi = (float)vv[c];
         float lo = (float)(vv[c] - (double)hi);
         fs[(3 + c) * n + s] = hi;
@@ -98,7 +104,7 @@ __global__ void store_mixed_kernel(int64_t n, const int32_t* __restrict__ ci, co
         for (int c = 0; c < 3; ++c) w[c] *= ig;
     }
     for (int c = 0; c < 3; ++c) {
-        if (r) r[3 * row + c] = G.lo[c] + ((double)ci[c * n + s] + (double)fs[c * n + s]) * G.d[c];
+        if (r) r[3 * row + c] = G.lo[c] + ((double)ci[c * n + s] + ((double)fs[c * n + s] + (double)fs[(9 + c) * n + s])) * G.d[c];
         if (v) v[3 * row + c] = w[c];
     }
 }

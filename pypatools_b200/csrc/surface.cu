@@ -79,7 +79,12 @@ extern "C" int ppt_surface_create(int64_t n_vertices, const double* vertices, in
     grid_for_mesh(lo, hi, n_triangles, S.dev.lo, h, S.dev.dims);
     for (int a = 0; a < 3; ++a) S.dev.inv_h[a] = 1.0 / h[a];
     const int64_t cells = (int64_t)S.dev.dims[0] * S.dev.dims[1] * S.dev.dims[2];
-    // bin each triangle into the cells its bounding box overlaps (count, then fill)
+    // bin each triangle into the cells its bounding box overlaps (count, then fill).
+    // The box is padded by 1e-7 of a cell: the segment and ray tests work on
+    // v0, e1 = v1 - v0, e2 = v2 - v0 rounded, whose hits can lie an ulp or so
+    // outside the vertices' box; a triangle within the pad of a cell face is
+    // listed on both sides of it, so no such hit falls in a cell that does not
+    // list the triangle (the tests stay the same as testing every triangle).
     auto cell_range = [&](int64_t t, int a, int* c0, int* c1) {
         double mn = INFINITY, mx = -INFINITY;
         for (int c = 0; c < 3; ++c) {
@@ -87,7 +92,8 @@ extern "C" int ppt_surface_create(int64_t n_vertices, const double* vertices, in
             mn = std::min(mn, x);
             mx = std::max(mx, x);
         }
-        const double u0 = (mn - S.dev.lo[a]) * S.dev.inv_h[a], u1 = (mx - S.dev.lo[a]) * S.dev.inv_h[a];
+        const double pad = 1e-7 / S.dev.inv_h[a];
+        const double u0 = (mn - pad - S.dev.lo[a]) * S.dev.inv_h[a], u1 = (mx + pad - S.dev.lo[a]) * S.dev.inv_h[a];
         *c0 = std::min(std::max((int)std::floor(u0), 0), S.dev.dims[a] - 1);
         *c1 = std::min(std::max((int)std::floor(u1), 0), S.dev.dims[a] - 1);
     };

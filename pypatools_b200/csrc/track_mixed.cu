@@ -25,8 +25,9 @@ struct MixCtx {
     const TrackMixDev* P;
     double phase;            // omega t0 + phi_i
     unsigned hits;
-    float c0, s0;            // cos, sin of the phase
-    const float2* tab;       // (cos, sin) of g omega dt for every g of the launch, or NULL
+    float c0h, c0l;          // cos of the phase as a float pair
+    float s0h, s0l;          // sin of the phase as a float pair
+    const float4* tab;       // (cos, sin, their low parts) of g omega dt for every g of the launch, or NULL
     int64_t tab0;            // the launch's first step
 };
 
@@ -34,56 +35,50 @@ struct MixCtx {
 // its map are ~100 steps; longer launches compute the same values directly.
 constexpr int kRfTable = 512;
 
-// Components a record layout can make non-zero: bit a of e_bits (b_bits)
-// is E_a (B_a); the six-component layout also carries the constant parts.
-// x * 0 and x + 0 are not identities in IEEE arithmetic (NaN, signed
-// zeros), so the compiler keeps every operation on a component that is
-// zero by construction unless the code leaves it out: the Boris kernels
-// below do, at compile time, from these masks.
-constexpr int e_bits(int L) { return L & 7; }
-constexpr int b_bits(int L) { return (L >> 3) & 7; }
-constexpr bool bit(int m, int a) { return ((m >> a) & 1) != 0; }
-// components of p x q that can be non-zero when q has the components of qm
-constexpr int cross_bits(int qm) {
-    return ((bit(qm, 1) || bit(qm, 2)) ? 1 : 0) | ((bit(qm, 2) || bit(qm, 0)) ? 2 : 0) |
-           ((bit(qm, 0) || bit(qm, 1)) ? 4 : 0);
-}
-// velocity components a Boris step can change under layout L
-constexpr int boris_bits(int L) { return e_bits(L) | cross_bits(b_bits(L)); }
-
 // (cos, sin) of g omega dt in float64: the per-step factor of the RF phase,
 // the same for every particle, so a block tabulates it once per launch.
 __device__ __forceinline__ void rf_turn(int64_t g, double wdt, double& cg, double& sg) {
     sincos((double)g * wdt, &sg, &cg);
 }
 
+// A float64 value as a float pair (head, rest).
+__device__ __forceinline__ float2 split_d(double x) {
+    const float h = (float)x;
+    return make_float2(h, (float)(x - (double)h));
+}
+
+// (cos, sin) of g omega dt and their low parts, from float64
+__device__ __forceinline__ float4 rf_turn_pair(int64_t g, double wdt) {
+    double cg, sg;
+    rf_turn(g, wdt, cg, sg);
+    const float2 c = split_d(cg), s = split_d(sg);
+    return make_float4(c.x, s.x, c.y, s.y);
+}
+
 // cos(omega (t0 + g dt) + phi_i) = cos(a + b) = cos a cos b - sin a sin b
-// with a = omega t0 + phi_i per particle and b = g omega dt per step: both
-// angles' cosines and sines are formed in float64 and rounded to float32,
-// then combined by one float32 product and one FMA (within 1.4e-7 of the
-// cosine, rms 2.8e-8).  The value depends on g and the particle only, table
-// or not, so tracks split into launches differently agree bit for bit.  A
-// launch's table covers every step it evaluates (step0 .. step0 + nsteps).
-__device__ __forceinline__ float rf_cos(const MixCtx& c, int64_t g) {
-    float2 t;
-    if (c.tab != nullptr) {
-        t = c.tab[(int)(g - c.tab0)];
-    } else {
-        double cg, sg;
-        rf_turn(g, c.P->wdt, cg, sg);
-        t = make_float2((float)cg, (float)sg);
-    }
-    return fmaf(c.c0, t.x, -(c.s0 * t.y));
+// with a = omega t0 + phi_i per particle and b = g omega dt per step, as a
+// float pair good to ~1e-13: both angles' cosines and sines are formed in
+// float64 and kept as float pairs, the two products split exactly (FMA) and
+// their difference by Knuth's two-sum.  A float32 factor would round at
+// 2.8e-8 rms per step, which the E kick carries into every velocity.  The
+// value depends on g and the particle only, table or not, so tracks split
+// into launches differently agree bit for bit.  A launch's table covers every
+// step it evaluates (step0 .. step0 + nsteps).
+__device__ __forceinline__ float2 rf_cos(const MixCtx& c, int64_t g) {
+    const float4 t = c.tab != nullptr ? c.tab[(int)(g - c.tab0)] : rf_turn_pair(g, c.P->wdt);
+    const float p = c.c0h * t.x, pe = fmaf(c.c0h, t.x, -p);
+    const float q = c.s0h * t.y, qe = fmaf(c.s0h, t.y, -q);
+    const float h = p - q;
+    const float bb = h - p;
+    const float err = (p - (h - bb)) + (-q - bb);
+    const float lo = (err + (pe - qe)) + (fmaf(c.c0h, t.z, c.c0l * t.x) - fmaf(c.s0h, t.w, c.s0l * t.y));
+    return make_float2(h, lo);
 }
 
 // Fill the block's RF table for steps step0 .. step0 + n - 1 (all threads
 // of the block call it; n <= kRfTable).
-__device__ __forceinline__ void build_rf_table(float2* tab, int64_t step0, int n, double wdt) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        double cg, sg;
-        rf_turn(step0 + i, wdt, cg, sg);
-        tab[i] = make_float2((float)cg, (float)sg);
-    }
+__device__ __forceinline__ void build_rf_table(float4* tab, int64_t step0, int n, double wdt) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tab[i] = rf_turn_pair(step0 + i, wdt);
     __syncthreads();
 }
 
@@ -114,14 +109,37 @@ __device__ __forceinline__ float2 tri8_pair(const float2 q[8], float2 tx, float2
     return lerp2(lerp2(c00, c10, ty), lerp2(c01, c11, ty), tz);
 }
 
+// tri8_pair whose last (z) level is split exactly: the result as (head,
+// tail) per lane.  The x and y levels round as in tri8_pair; the z level --
+// head = c0 + t (c1 - c0) -- rounds at half an ulp of the field, which for a
+// map that varies along z is the largest rounding of the interpolation and
+// reaches every velocity through the kick, so it is kept: t (c1 - c0) split
+// by an FMA, the sum by Knuth's two-sum.
+__device__ __forceinline__ float2 tri8_pair_ff(const float2 q[8], float2 tx, float2 ty, float2 tz, float2& lo) {
+    const float2 c00 = lerp2(q[0], q[4], tx), c01 = lerp2(q[1], q[5], tx);
+    const float2 c10 = lerp2(q[2], q[6], tx), c11 = lerp2(q[3], q[7], tx);
+    const float2 c0 = lerp2(c00, c10, ty), c1 = lerp2(c01, c11, ty);
+    const float2 d = sub2(c1, c0);
+    const float2 p = __fmul2_rn(tz, d);
+    const float2 pe = fma2(tz, d, make_float2(-p.x, -p.y));
+    const float2 h = __fadd2_rn(c0, p);
+    const float2 bb = sub2(h, c0);
+    const float2 e = __fadd2_rn(sub2(c0, sub2(h, bb)), sub2(p, bb));
+    lo = __fadd2_rn(e, pe);
+    return h;
+}
+
 // Trilinear E/B at (cell, offset) from the float32 map of record layout L;
 // returns false when outside.  Components L does not store are compile-time
 // zeros, so the arithmetic that would multiply them vanishes from the
 // kernel.  Only the six-component layout carries the constant field parts
 // (the host creates that layout whenever they are not zero).
+// El: the low parts of E's components (tri8_pair_ff).
+// fl: the offset's low words (zeros where only the high words are known).
 template <int L>
-__device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3], F3& E,
-                                             F3& B) {
+__device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3],
+                                             const float fl[3], F3& E, F3& B, F3& El) {
+    El = f3(0.0f, 0.0f, 0.0f);
     if constexpr (L == kLayFull) {
         E = f3(P.e_const[0], P.e_const[1], P.e_const[2]);
         B = f3(P.b_const[0], P.b_const[1], P.b_const[2]);
@@ -131,9 +149,9 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
     }
     int i, j, k;
     float tx, ty, tz;
-    if (!mixed_axis(cell[0], f[0], P.G.n[0], i, tx)) return false;
-    if (!mixed_axis(cell[1], f[1], P.G.n[1], j, ty)) return false;
-    if (!mixed_axis(cell[2], f[2], P.G.n[2], k, tz)) return false;
+    if (!mixed_axis(cell[0], f[0], fl[0], P.G.n[0], i, tx)) return false;
+    if (!mixed_axis(cell[1], f[1], fl[1], P.G.n[1], j, ty)) return false;
+    if (!mixed_axis(cell[2], f[2], fl[2], P.G.n[2], k, tz)) return false;
     const MapDev& m = P.map;
     const float2 tx2 = make_float2(tx, tx), ty2 = make_float2(ty, ty), tz2 = make_float2(tz, tz);
     constexpr int W = layout_width(L);
@@ -167,15 +185,17 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
             ldg_f32x8(pc[c], q[2 * c]);
             ldg_f32x8(pc[c] + 8, q[2 * c + 1]);
         }
-        float2 o[4];
+        float2 o[4], ol[2];
 #pragma unroll
         for (int h = 0; h < 4; ++h) {
             float2 qp[8];
 #pragma unroll
             for (int c = 0; c < 8; ++c) qp[c] = make_float2(q[c][2 * h], q[c][2 * h + 1]);
-            o[h] = tri8_pair(qp, tx2, ty2, tz2);
+            if (h < 2) o[h] = tri8_pair_ff(qp, tx2, ty2, tz2, ol[h]);
+            else o[h] = tri8_pair(qp, tx2, ty2, tz2);
         }
         E = E + f3(o[0].x, o[0].y, o[1].x);
+        El = f3(ol[0].x, ol[0].y, ol[1].x);
         B = B + f3(o[2].x, o[2].y, o[3].x);
     } else if constexpr (W == 4) {
         // three packed components and a pad: one 128-bit load per corner, two pairs
@@ -191,11 +211,19 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
             qa[c] = make_float2(q[c].x, q[c].y);
             qb[c] = make_float2(q[c].z, q[c].w);
         }
-        const float2 oa = tri8_pair(qa, tx2, ty2, tz2), ob = tri8_pair(qb, tx2, ty2, tz2);
-        if constexpr (L == kLayE) E = f3(oa.x, oa.y, ob.x);
-        else if constexpr (L == kLayB) B = f3(oa.x, oa.y, ob.x);
-        else {   // kLayExEyBz
+        if constexpr (L == kLayE) {
+            float2 la, lb;
+            const float2 oa = tri8_pair_ff(qa, tx2, ty2, tz2, la), ob = tri8_pair_ff(qb, tx2, ty2, tz2, lb);
+            E = f3(oa.x, oa.y, ob.x);
+            El = f3(la.x, la.y, lb.x);
+        } else if constexpr (L == kLayB) {
+            const float2 oa = tri8_pair(qa, tx2, ty2, tz2), ob = tri8_pair(qb, tx2, ty2, tz2);
+            B = f3(oa.x, oa.y, ob.x);
+        } else {   // kLayExEyBz
+            float2 la;
+            const float2 oa = tri8_pair_ff(qa, tx2, ty2, tz2, la), ob = tri8_pair(qb, tx2, ty2, tz2);
             E = f3(oa.x, oa.y, 0.0f);
+            El = f3(la.x, la.y, 0.0f);
             B = f3(0.0f, 0.0f, ob.x);
         }
     } else if constexpr (W == 2) {
@@ -206,8 +234,10 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
             q[2 * c] = __ldg(reinterpret_cast<const float2*>(pc[c]));
             q[2 * c + 1] = __ldg(reinterpret_cast<const float2*>(pc[c] + 2));
         }
-        const float2 o = tri8_pair(q, tx2, ty2, tz2);
+        float2 ol;
+        const float2 o = tri8_pair_ff(q, tx2, ty2, tz2, ol);
         E = f3(0.0f, 0.0f, o.x);
+        El = f3(0.0f, 0.0f, ol.x);
         B = f3(0.0f, 0.0f, o.y);
     } else {
         // kLayBz: one 32-bit load per corner
@@ -231,16 +261,25 @@ __device__ __forceinline__ bool const_fields(const TrackMixDev& P) {
 
 // Fields at the step's field time t0 + g dt (+ toff for RK4 stages); the
 // float64 time and phase are formed only when E is non-zero.
+// (head, tail) of (ch + cl)(eh + el), the product split exactly
+__device__ __forceinline__ void mul_pair(float ch, float cl, float& eh, float& el) {
+    const float h = ch * eh;
+    el = fmaf(ch, eh, -h) + fmaf(ch, el, cl * eh);
+    eh = h;
+}
+
+// El: the low parts of E's components (the interpolation's last level and,
+// with RF, the factor's and the product's), for the Boris kick correction.
 template <bool RF, int L>
-__device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], int64_t g,
-                                             double toff, F3& E, F3& B) {
-    bool in = gather_mixed<L>(*c.P, cell, f, E, B);
+__device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], const float fl[3],
+                                             int64_t g, double toff, F3& E, F3& B, F3& El) {
+    bool in = gather_mixed<L>(*c.P, cell, f, fl, E, B, El);
     c.hits += in;
     if (RF) {
         constexpr int EM = e_bits(L);
         if ((bit(EM, 0) && E.x != 0.0f) || (bit(EM, 1) && E.y != 0.0f) || (bit(EM, 2) && E.z != 0.0f)) {
             // omega (t0 + g dt + toff) + phi_i = (omega t0 + phi_i) + g (omega dt) + omega toff, in float64
-            float cf;
+            float2 cf;
             if (toff == 0.0) {
                 cf = rf_cos(c, g);
             } else {
@@ -250,15 +289,24 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
                 double ph = fma((double)g, c.P->wdt, c.phase);
                 ph = fma(c.P->omega, toff, ph);
                 const double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
-                cf = cosf((float)red);
+                cf = make_float2(cosf((float)red), 0.0f);
             }
-            if constexpr (bit(EM, 0)) E.x = cf * E.x;
-            if constexpr (bit(EM, 1)) E.y = cf * E.y;
-            if constexpr (bit(EM, 2)) E.z = cf * E.z;
+            if constexpr (bit(EM, 0)) mul_pair(cf.x, cf.y, E.x, El.x);
+            if constexpr (bit(EM, 1)) mul_pair(cf.x, cf.y, E.y, El.y);
+            if constexpr (bit(EM, 2)) mul_pair(cf.x, cf.y, E.z, El.z);
         }
     }
     return in || const_fields<L>(*c.P);
 }
+
+// The same without the low parts (the pushers other than the Boris family's).
+template <bool RF, int L>
+__device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], const float fl[3],
+                                             int64_t g, double toff, F3& E, F3& B) {
+    F3 El;
+    return fields_mixed<RF, L>(c, cell, f, fl, g, toff, E, B, El);
+}
+
 
 // Boris velocity increment in float32 (pusher.py:149-163 rearranged):
 // v_new - v = 2 a + (v- + v- x t) x s,  a = (q/m) E dt/2,  v- = v + a,
@@ -405,6 +453,38 @@ __device__ __forceinline__ void vel_add_fast(float vh[3], float vl[3], F3 d, flo
     }
 }
 
+// The E kick's low-word correction: 2 ((q/m) dt/2 E exactly - its float32
+// product) for the components of EM, from E's low parts El (fields_mixed).
+template <int EM>
+__device__ __forceinline__ F3 kick_correction(F3 E, F3 El, float hqdt) {
+    const float e[3] = {E.x, E.y, E.z}, el[3] = {El.x, El.y, El.z};
+    float k[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (bit(EM, i)) {
+            const float a = hqdt * e[i];
+            k[i] = 2.0f * (fmaf(hqdt, e[i], -a) + hqdt * el[i]);
+        } else {
+            k[i] = 0.0f;
+        }
+    }
+    return f3(k[0], k[1], k[2]);
+}
+
+// vel_add_fast with the kick correction kc added to the low word.
+template <int M>
+__device__ __forceinline__ void vel_add_fast_kc(float vh[3], float vl[3], F3 d, float ws, F3 kc) {
+    const float dd[3] = {d.x, d.y, d.z}, kk[3] = {kc.x, kc.y, kc.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (!bit(M, a)) continue;
+        const float s = vh[a] + dd[a];
+        const float err = dd[a] - (s - vh[a]);
+        vl[a] = fmaf(dd[a], ws, (vl[a] + err) + kk[a]);
+        vh[a] = s;
+    }
+}
+
 template <int M>
 __device__ __forceinline__ void vel_renorm(float vh[3], float vl[3]) {
 #pragma unroll
@@ -422,10 +502,200 @@ __device__ __forceinline__ void vel_set(float vh[3], float vl[3], F3 v) {
     vl[0] = vl[1] = vl[2] = 0.0f;
 }
 
-__device__ __forceinline__ void advance(const TrackMixDev& P, int cell[3], float f[3], const float vh[3],
+// Per-step position increment v dt / d in cell units, recomputed only when
+// the velocity changes, as (q, r): q = the increment rounded to a multiple
+// of 2^-22 cells, r the rest (v = vh + vl, dt / d = kh + kl; r is formed from
+// the exact residual of vh kh - q by an FMA).  The offset's high word is a
+// multiple of 2^-22 in [0, 1] in a map, so hi + q is exact there for steps
+// below three cells (|hi + q| < 4: add_cells_q).
+__device__ __forceinline__ void split_q(float p, float vh, float vl, float kh, float kl, float& q, float& r) {
+    q = rintf(p * 0x1p22f) * 0x1p-22f;
+    r = fmaf(vh, kh, -q) + fmaf(vh, kl, vl * kh);
+}
+
+// ---------------------------------------------------------------------------
+// u-state Boris family of the mixed form: relativistic Boris and Vay (2008)
+// on u = gamma v (the float64 form's boris_rel_u / vay_u).  The increment of
+// u is formed in float32 as for the Boris above; gamma enters through its
+// reciprocal as a float pair (ih + il) good to ~1e-14, because a float32
+// gamma would round the same way at every step of a gyration (|u| constant):
+// a fixed bias of the rotation angle and of the speed.  The rotation part of
+// an increment is scaled by (1 + il / ih), like the (1 + ws) scaling of the
+// float32 q dt / 2m, through the velocity's low word.
+// ---------------------------------------------------------------------------
+constexpr float kInvC2f = 1.1126500560536184e-17f;   // 1 / c^2 [s^2/m^2]
+
+// u.u / c^2 of the float32 head of u (its rounding varies from step to step)
+__device__ __forceinline__ float u2_over_c2(const float u[3]) {
+    return fmaf(u[0], u[0], fmaf(u[1], u[1], u[2] * u[2])) * kInvC2f;
+}
+
+// 1 / sqrt(gh + gl) as a float pair: an rsqrt estimate and one Newton step
+// whose residual 1 - g i0^2 is formed from exact products (m is within a few
+// ulps of 1, so 1 - m is exact).
+__device__ __forceinline__ void inv_sqrt_pair(float gh, float gl, float& ih, float& il) {
+    const float i0 = rsqrtf(gh);
+    const float p = i0 * i0, pe = fmaf(i0, i0, -p);
+    const float m = gh * p, me = fmaf(gh, p, -m);
+    const float r = ((1.0f - m) - me) - fmaf(gh, pe, gl * p);
+    ih = i0;
+    il = 0.5f * i0 * r;
+}
+
+// 1 / gamma = 1 / sqrt(1 + x), with 1 + x split exactly (Knuth's two-sum):
+// for the small x of ions 1 + x alone would round identically at every step.
+__device__ __forceinline__ void inv_gamma_pair(float x, float& ih, float& il) {
+    const float gh = 1.0f + x;
+    const float bb = gh - 1.0f;
+    const float gl = (1.0f - (gh - bb)) + (x - bb);
+    inv_sqrt_pair(gh, gl, ih, il);
+}
+
+// Relativistic Boris increment of u (boris_rel_u in the float64 form):
+// a = (q/m) E dt/2, u- = u + a, t = (q/m) B dt/2 / gamma(u-), s = 2 t / (1 + t.t),
+// du = 2 a + (u- + u- x t) x s; corr: the low-word correction of du
+// (ws for the float32 q dt / 2m, il / ih for gamma's low part, rotation only).
+template <int EM, int BM>
+__device__ __forceinline__ void boris_rel_du(const float u[3], F3 E, F3 B, float hqdt, float ws, float du[3],
+                                             float corr[3]) {
+    constexpr int CM = cross_bits(BM);
+    const float e[3] = {E.x, E.y, E.z}, b[3] = {B.x, B.y, B.z};
+    float a[3], um[3], t[3], sv[3], up[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        a[i] = bit(EM, i) ? hqdt * e[i] : 0.0f;
+        um[i] = bit(EM, i) ? u[i] + a[i] : u[i];
+    }
+    float ih, il;
+    inv_gamma_pair(u2_over_c2(um), ih, il);
+    const float th = hqdt * ih;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) t[i] = bit(BM, i) ? th * b[i] : 0.0f;
+    float tt = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (bit(BM, i)) tt = fmaf(t[i], t[i], tt);
+    const float sf = __fdividef(2.0f, 1.0f + tt);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) sv[i] = bit(BM, i) ? sf * t[i] : 0.0f;
+    up[0] = bit(CM, 0) ? um[0] + cross_m<BM, 0>(um, t) : um[0];
+    up[1] = bit(CM, 1) ? um[1] + cross_m<BM, 1>(um, t) : um[1];
+    up[2] = bit(CM, 2) ? um[2] + cross_m<BM, 2>(um, t) : um[2];
+    const float rot[3] = {cross_m<BM, 0>(up, sv), cross_m<BM, 1>(up, sv), cross_m<BM, 2>(up, sv)};
+    const float wr = ws + __fdividef(il, ih);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float kick = bit(EM, i) ? 2.0f * a[i] : 0.0f;
+        const float r = bit(CM, i) ? rot[i] : 0.0f;
+        du[i] = kick + r;
+        corr[i] = fmaf(r, wr, kick * ws);
+    }
+}
+
+// Vay (2008) increment of u (vay_u in the float64 form):
+// u' = u + (q/m) dt (E + v x B / 2) with v = u / gamma(u); tau = (q/m) B dt/2;
+// gamma_new^2 = G = (sigma + sqrt(sigma^2 + 4 (tau^2 + (u'.tau / c)^2))) / 2,
+// sigma = 1 + u'^2/c^2 - tau^2 (both as float pairs); t = tau / gamma_new,
+// s = 1 / (1 + t^2); u_new = s (u' + (u'.t) t + u' x t), written as the
+// increment du = (u' - u) + s ((u'.t) t + u' x t - t^2 u').
+template <int EM, int BM>
+__device__ __forceinline__ void vay_du(const float u[3], F3 E, F3 B, float hqdt, float ws, float du[3],
+                                       float corr[3]) {
+    const float e[3] = {E.x, E.y, E.z}, b[3] = {B.x, B.y, B.z};
+    float ih, il;
+    inv_gamma_pair(u2_over_c2(u), ih, il);
+    const float v[3] = {u[0] * ih, u[1] * ih, u[2] * ih};
+    const float vxb[3] = {cross_m<BM, 0>(v, b), cross_m<BM, 1>(v, b), cross_m<BM, 2>(v, b)};
+    float d1[3], up[3], tau[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        // (q/m) dt (E + v x B / 2) = 2 hqdt E + hqdt (v x B)
+        const float ke = bit(EM, i) ? 2.0f * hqdt * e[i] : 0.0f;
+        const float kb = hqdt * vxb[i];
+        d1[i] = ke + kb;
+        up[i] = u[i] + d1[i];
+        tau[i] = bit(BM, i) ? hqdt * b[i] : 0.0f;
+        corr[i] = fmaf(kb, __fdividef(il, ih), d1[i] * ws);
+    }
+    float tau2 = 0.0f, ut = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (bit(BM, i)) {
+            tau2 = fmaf(tau[i], tau[i], tau2);
+            ut = fmaf(up[i], tau[i], ut);
+        }
+    const float us = ut * (1.0f / kCf);
+    const float w = fmaf(us, us, tau2);                      // tau^2 + u*^2
+    // sigma = 1 + x' - tau^2 as a pair
+    const float x = u2_over_c2(up);
+    const float sh0 = 1.0f + x, bb = sh0 - 1.0f;
+    const float sl0 = (1.0f - (sh0 - bb)) + (x - bb);
+    const float sh = sh0 - tau2;                             // tau^2 << 1: exact to the pair
+    const float sl = sl0 - ((sh - sh0) + tau2);
+    // D = sigma^2 + 4 w as a pair, sqrt(D) as a pair
+    const float d0 = sh * sh, d0e = fmaf(sh, sh, -d0);
+    const float dh = fmaf(4.0f, w, d0);
+    const float dl = ((d0 - dh) + 4.0f * w) + fmaf(2.0f * sh, sl, d0e);
+    const float rd = sqrtf(dh);
+    const float rr = rd * rd, rre = fmaf(rd, rd, -rr);
+    const float rdl = __fdividef(((dh - rr) - rre) + dl, 2.0f * rd);
+    // G = (sigma + sqrt D) / 2, then 1 / gamma_new = 1 / sqrt(G)
+    const float gh = 0.5f * (sh + rd);
+    const float gl = 0.5f * (((sh - 2.0f * gh) + rd) + (sl + rdl));
+    float jh, jl;
+    inv_sqrt_pair(gh, gl, jh, jl);
+    float t[3];
+    float tt = 0.0f, upt = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        t[i] = bit(BM, i) ? tau[i] * jh : 0.0f;
+        if (bit(BM, i)) {
+            tt = fmaf(t[i], t[i], tt);
+            upt = fmaf(up[i], t[i], upt);
+        }
+    }
+    const float sf = __fdividef(1.0f, 1.0f + tt);
+    const float wr = ws + __fdividef(jl, jh);
+    const float uxt[3] = {cross_m<BM, 0>(up, t), cross_m<BM, 1>(up, t), cross_m<BM, 2>(up, t)};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float rot = sf * (fmaf(upt, t[i], uxt[i]) - tt * up[i]);
+        du[i] = d1[i] + rot;
+        corr[i] = fmaf(rot, wr, corr[i]);
+    }
+}
+
+// u += du with its correction: a fast two-sum into the low word, renormalised
+// with the other Boris steps after global steps g with (g + 1) % 4 == 0.
+__device__ __forceinline__ void vel_add_corr(float vh[3], float vl[3], const float du[3], const float corr[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float s = vh[a] + du[a];
+        const float err = du[a] - (s - vh[a]);
+        vl[a] = (vl[a] + err) + corr[a];
+        vh[a] = s;
+    }
+}
+
+// Position increment (dh + dl) = (u / gamma(u)) dt / d of the u state, with
+// 1 / gamma as a pair and the products split exactly.
+__device__ __forceinline__ void increment_u(const TrackMixDev& P, const float uh[3], const float ul[3], float dh[3],
+                                            float dl[3]) {
+    float ih, il;
+    inv_gamma_pair(u2_over_c2(uh), ih, il);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float p = uh[a] * ih;
+        const float pe = fmaf(uh[a], ih, -p);
+        const float pl = fmaf(uh[a], il, fmaf(ul[a], ih, pe));   // v = p + pl
+        split_q(p * P.kh[a], p, pl, P.kh[a], P.kl[a], dh[a], dl[a]);
+    }
+}
+
+__device__ __forceinline__ void advance(const TrackMixDev& P, int cell[3], float f[3], float fl[3], const float vh[3],
                                         const float vl[3]) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) advance_axis(cell[a], f[a], vh[a], vl[a], P.kh[a], P.kl[a]);
+    for (int a = 0; a < 3; ++a) advance_axis(cell[a], f[a], fl[a], vh[a], vl[a], P.kh[a], P.kl[a]);
 }
 
 // Cell + offset of the point (cell, f) + d (d in metres), for RK4 stages.
@@ -442,22 +712,37 @@ __device__ __forceinline__ void offset_point(const TrackMixDev& P, const int cel
     }
 }
 
-// Per-step position increment v dt / d in cell units as a float-float pair,
-// recomputed only when the velocity changes.
 template <int M = 7>
 __device__ __forceinline__ void increment(const TrackMixDev& P, const float vh[3], const float vl[3], float dh[3],
                                           float dl[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         if (!bit(M, a)) continue;
-        float p = vh[a] * P.kh[a];
-        float e = fmaf(vh[a], P.kh[a], -p);
-        dh[a] = p;
-        dl[a] = fmaf(vh[a], P.kl[a], fmaf(vl[a], P.kh[a], e));
+        split_q(vh[a] * P.kh[a], vh[a], vl[a], P.kh[a], P.kl[a], dh[a], dl[a]);
     }
 }
 
-// Per-particle loop state of the Boris family: the position increment.
+// (cell, hi + lo) += q + r cells for the Boris family's steps that may see a
+// field: hi + q exact (both multiples of 2^-22 and |hi + q| < 4), r into lo;
+// with `fold` (after global steps g with (g + 1) % 4 == 0) lo's whole
+// multiples of 2^-22 move into hi (exact), so hi stays within ~2^-23 of the
+// position (the faces are decided on hi + lo: mixed_axis); whole cells out of
+// hi (exact).  Leaves hi in [0, 1).
+__device__ __forceinline__ void add_cells_q(float& cell, float& hi, float& lo, float q, float r, bool fold) {
+    float h = hi + q;
+    lo += r;
+    if (fold) {
+        const float qq = rintf(lo * 0x1p22f) * 0x1p-22f;
+        h += qq;
+        lo -= qq;
+    }
+    const float cc = floorf(h);
+    hi = h - cc;
+    cell += cc;
+}
+
+// Per-particle loop state of the Boris family: the position increment, the
+// (q, r) pair of increment() / increment_u().
 struct Drift {
     float dh[3];
     float dl[3];
@@ -465,69 +750,157 @@ struct Drift {
 
 // Field-free steps of the Boris family (Boris, leapfrog).  Outside the map
 // with no constant field both updates leave v exactly unchanged (every added
-// term is zero), so such a step is the position advance by the high part of
-// the increment alone (the low part is a 3e-8 relative correction of the
-// displacement).  The whole-cell carry is taken after global steps g with
-// (g + 1) % 4 == 0 only; in between the offset runs up to 1 + 4 |dh| cells.
-// Because the carry points depend on the global step index alone, a track
-// gives the same bits however its steps are split into launches, runs or
-// serving ticks.  Normalising (cf + floor f, f - floor f) is exact, so the
-// represented position never depends on it.
-__device__ __forceinline__ void carry(float cf[3], float f[3]) {
+// term is zero), so such a step is the position advance alone.  The offset
+// is a (hi, lo) pair per axis; a field-free step adds the drift quanta (q, r)
+// of the increment (drift_quanta) to it with one packed FADD2, and hi + q is
+// exact, so the drift does not round the position step after step.  The
+// whole-cell carry is taken after global steps g with (g + 1) % kCarry == 0
+// only; in between hi runs up to 1 + kCarry |dh| cells.  Because the carry
+// points depend on the global step index alone, a track gives the same bits
+// however its steps are split into launches, runs or serving ticks.
+// Normalising a non-negative hi (cf + floor hi, hi - floor hi) is exact, and
+// so is it for a negative hi that is a multiple of the quantum.
+constexpr int kCarry = 32;
+constexpr unsigned kCarryMask = kCarry - 1;
+
+// The increment (dh + dl) of field-free steps as q + r: q the increment
+// rounded to a multiple of u, the float32 spacing at the largest |hi| a carry
+// period reaches (|hi| < 2 + kCarry |dh|); r = (dh - q) + dl the rest,
+// rounded to a multiple of u 2^-19.  Once hi is a multiple of u (after at
+// most a few roundings at the start of a drift), hi + q is exact; and the low
+// word, a multiple of u 2^-19 below 32 u (the carry keeps it below
+// (kCarry + 1) u / 2 = 16.5 u), is changed by exact additions only, so
+// whether r is added at every step or kCarry r at a carry point gives the
+// same bits.  Without the split, the float32 sum hi + dh rounds dh to the
+// spacing of hi's binade, the same amount every step: a fixed-sign error of
+// up to 2^-23 cells per step; the rounding of r costs at most u 2^-20 per
+// step (1e-12 of a cell for the RF-gap protons).  U[a] = (u, 1 / u) per axis,
+// for the carries.
+__device__ __forceinline__ void drift_quanta(const Drift& d, float2 Q[3], float2 U[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float cc = floorf(f[a]);
-        f[a] -= cc;
+        const float bound = fmaf((float)kCarry, fabsf(d.dh[a]), 2.0f);
+        const int eb = (__float_as_int(bound) >> 23) & 0xff;   // bound in [2^(eb-127), 2^(eb-126))
+        const float u = __int_as_float((eb - 23) << 23);        // float32 spacing below 2^(eb-126)
+        const float ui = __int_as_float((277 - eb) << 23);      // 1 / u (both powers of two)
+        const float q = rintf(d.dh[a] * ui) * u;
+        const float r = (d.dh[a] - q) + d.dl[a];
+        const float w = __int_as_float((eb - 42) << 23);        // u 2^-19
+        const float wi = __int_as_float((296 - eb) << 23);      // 1 / w
+        Q[a] = make_float2(q, rintf(r * wi) * w);
+        U[a] = make_float2(u, ui);
+    }
+}
+
+// The carry of field-free steps: whole cells out of the high word, and the
+// whole quanta the low word has gathered (N r after N steps) into it, so the
+// high word -- which the cell pre-test and the trilinear weight read --
+// stays within u of the position.  Both moves are exact.
+__device__ __forceinline__ void carry(float cf[3], float2 o[3], const float2 U[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float cc = floorf(o[a].x);
+        o[a].x -= cc;
+        cf[a] += cc;
+        const float qq = rintf(o[a].y * U[a].y) * U[a].x;
+        o[a].x += qq;
+        o[a].y -= qq;
+    }
+}
+
+// Bring the offset pair onto the drift's grids: hi a multiple of u (its
+// finer bits go to lo), lo a multiple of u 2^-19 (rounded, ~1e-13 of a cell,
+// once after each stretch in the map).  Idempotent: once on the grids a pair
+// stays there (every drift operation is exact), so a call at the start of
+// every run changes nothing but the first, and a track's bits do not depend
+// on where its runs start.
+__device__ __forceinline__ void drift_enter(float2 o[3], const float2 U[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float u = U[a].x, ui = U[a].y;
+        const float hq = rintf(o[a].x * ui) * u;
+        float lo = o[a].y + (o[a].x - hq);
+        const float w = u * 0x1p-19f, wi = ui * 0x1p19f;
+        o[a].x = hq;
+        o[a].y = rintf(lo * wi) * w;
+    }
+}
+
+__device__ __forceinline__ void add_quanta(float2 o[3], const float2 Q[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[a] = __fadd2_rn(o[a], Q[a]);
+}
+
+// Whole cells out of the high word (exact: hi is a multiple of u after the
+// drift's first steps, and hi - floor(hi) is exact for hi >= 0 anyway), so a
+// Boris-family step starts from hi in [0, 1] without normalising it first.
+__device__ __forceinline__ void normalise(float cf[3], float2 o[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float cc = floorf(o[a].x);
+        o[a].x -= cc;
         cf[a] += cc;
     }
 }
 
-__device__ __forceinline__ void add_dh(float f[3], const float dh[3]) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) f[a] += dh[a];
-}
-
-// m field-free steps from global step g0.
-__device__ __forceinline__ void drift_steps(float cf[3], float f[3], const float dh[3], int64_t g0, int m) {
+// m field-free steps from global step g0.  Inside whole carry periods the
+// high words take q at every step -- x and y as one packed FADD2, so a step
+// is two issue slots -- and the low words kCarry r at the carry point (exact,
+// so the same bits as r at every step, see drift_quanta).
+__device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const float2 Q[3], const float2 U[3],
+                                            int64_t g0, int m) {
+    drift_enter(o, U);
     int j = 0;
-    for (; j < m && ((unsigned)(g0 + j) & 3u) != 0u; ++j) {
-        add_dh(f, dh);
-        if (((unsigned)(g0 + j + 1) & 3u) == 0u) carry(cf, f);
+    for (; j < m && ((unsigned)(g0 + j) & kCarryMask) != 0u; ++j) {
+        add_quanta(o, Q);
+        if (((unsigned)(g0 + j + 1) & kCarryMask) == 0u) carry(cf, o, U);
     }
-    for (; j + 4 <= m; j += 4) {
-        add_dh(f, dh);
-        add_dh(f, dh);
-        add_dh(f, dh);
-        add_dh(f, dh);
-        carry(cf, f);
+    const float2 qxy = make_float2(Q[0].x, Q[1].x);
+    const float qz = Q[2].x;
+    for (; j + kCarry <= m; j += kCarry) {
+        float2 hxy = make_float2(o[0].x, o[1].x);
+        float hz = o[2].x;
+#pragma unroll
+        for (int k = 0; k < kCarry; ++k) {
+            hxy = __fadd2_rn(hxy, qxy);
+            hz += qz;
+        }
+        o[0].x = hxy.x;
+        o[1].x = hxy.y;
+        o[2].x = hz;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) o[a].y = fmaf((float)kCarry, Q[a].y, o[a].y);
+        carry(cf, o, U);
     }
-    for (; j < m; ++j) add_dh(f, dh);   // fewer than 4 steps from an aligned start: no carry point
+    for (; j < m; ++j) add_quanta(o, Q);   // fewer than kCarry steps from an aligned start: no carry point
+    normalise(cf, o);
 }
 
 // Steps the particle certainly stays outside the cell range of the map (the
 // pre-test of family_step), so that they are field-free drift steps: it is
 // outside on some axis and must travel `dist` cells at `rate` cells per step
-// to come back on that axis.  (cn, fn) is the normalised position.  Each drift
-// step moves the offset with a rounding error below 2^-24 (5 |dh| + 2) cells
-// (the offset stays below 1 + 4 |dh| between carries); that and the rounding
-// of this estimate are covered by the margin, so every step counted here is
-// one the pre-test would have sent down the drift branch.
+// to come back on that axis.  (cn, fn) is the normalised position and q the
+// per-step advance of the high word, which is all the pre-test sees; the
+// margin covers a rounding of 2^-24 ((kCarry + 1) |q| + 2) cells per step
+// and that of this estimate, so every step counted here is one the pre-test
+// would have sent down the drift branch.
 __device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cn[3], const float fn[3],
-                                           const float dh[3]) {
+                                           const float2 Q[3]) {
     float best = 0.0f;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         float dist, rate;
+        const float q = Q[a].x;
         if (cn[a] < 0.0f) {
             dist = -cn[a] - fn[a];                          // back in range once cn + fn >= 0
-            rate = dh[a];
+            rate = q;
         } else if (cn[a] > P.cell_max[a]) {
             dist = (cn[a] - (P.cell_max[a] + 1.0f)) + fn[a];   // back once cn + fn < cell_max + 1
-            rate = -dh[a];
+            rate = -q;
         } else {
             continue;
         }
-        const float k = rate > 0.0f ? dist / (rate + 1.2e-7f * fmaf(5.0f, fabsf(dh[a]), 2.0f)) : 2e9f;
+        const float k = rate > 0.0f ? dist / (rate + 1.2e-7f * fmaf((float)(kCarry + 1), fabsf(q), 2.0f)) : 2e9f;
         best = fmaxf(best, k);
     }
     best = fmaf(best, 0.99999f, -2.0f);
@@ -538,101 +911,108 @@ __device__ __forceinline__ int quiet_steps(const TrackMixDev& P, const float cn[
 // integers below 2^24).  Returns the number of following steps known to be
 // field-free (0 when this step met a field or the particle may come back).
 template <int ALG, bool RF, int L>
-__device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float f[3], float vh[3], float vl[3], Drift& d,
+__device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float2 o[3], float vh[3], float vl[3], Drift& d,
                                            int64_t g) {
     const TrackMixDev& P = *c.P;
-    float cn[3], fn[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float cc = floorf(f[a]);
-        cn[a] = cf[a] + cc;
-        fn[a] = f[a] - cc;
-    }
+    // (cf, hi) is normalised: hi in [0, 1] after steps that may see a field,
+    // after field-free runs and steps (normalise), and in the loaded state
+    const float cn[3] = {cf[0], cf[1], cf[2]};
+    const float fn[3] = {o[0].x, o[1].x, o[2].x};
     // cheap pre-test on the cell range (the last node layer included); the
     // exact bounds rule is applied inside gather_mixed
     const bool maybe = (cn[0] >= 0.0f) & (cn[0] <= P.cell_max[0]) & (cn[1] >= 0.0f) & (cn[1] <= P.cell_max[1]) &
                        (cn[2] >= 0.0f) & (cn[2] <= P.cell_max[2]);
     if (maybe || const_fields<L>(P)) {
         const int cell[3] = {(int)cn[0], (int)cn[1], (int)cn[2]};
-        F3 E, B;
-        if (fields_mixed<RF, L>(c, cell, fn, g, 0.0, E, B)) {
+        F3 E, B, El;
+        const float fln[3] = {o[0].y, o[1].y, o[2].y};
+        if (fields_mixed<RF, L>(c, cell, fn, fln, g, 0.0, E, B, El)) {
             F3 v = f3(vh[0], vh[1], vh[2]);
             if constexpr (ALG == PPT_ALG_BORIS) {
-                // only the velocity components the layout's fields can change
+                // only the velocity components the layout's fields can change;
+                // the kick's float32 roundings go to the low word
                 constexpr int DM = boris_bits(L);
-                vel_add_fast<DM>(vh, vl, boris_dv<L>(v, E, B, P.hqdt), P.wscale);
+                vel_add_fast_kc<DM>(vh, vl, boris_dv<L>(v, E, B, P.hqdt), P.wscale,
+                                    kick_correction<e_bits(L)>(E, El, P.hqdt));
                 if (((unsigned)(g + 1) & 3u) == 0u) vel_renorm<DM>(vh, vl);
                 increment<DM>(P, vh, vl, d.dh, d.dl);
+            } else if constexpr (ALG == PPT_ALG_BORIS_REL || ALG == PPT_ALG_VAY) {
+                // the state is u = gamma v; every component moves with gamma
+                float du[3], corr[3];
+                if constexpr (ALG == PPT_ALG_BORIS_REL)
+                    boris_rel_du<e_bits(L), b_bits(L)>(vh, E, B, P.hqdt, P.wscale, du, corr);
+                else
+                    vay_du<e_bits(L), b_bits(L)>(vh, E, B, P.hqdt, P.wscale, du, corr);
+                vel_add_corr(vh, vl, du, corr);
+                if (((unsigned)(g + 1) & 3u) == 0u) vel_renorm<7>(vh, vl);
+                increment_u(P, vh, vl, d.dh, d.dl);
             } else {
                 vel_add(vh, vl, P.dtf * lorentz_f(v, E, B, P.qm));
                 increment(P, vh, vl, d.dh, d.dl);
             }
         }
-        // where fields act (or may), the full float-float increment and a carry
+        // where fields act (or may): the increment (q, r) into the offset pair,
+        // nothing rounded away (add_cells_q); lo folds into hi with the
+        // velocity's renormalisation, after global steps g with (g + 1) % 4 == 0
+        const bool fold = ((unsigned)(g + 1) & 3u) == 0u;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float x = fn[a] + d.dh[a];
-            x = x + d.dl[a];
-            const float cc = floorf(x);
-            f[a] = x - cc;   // in [0, 1]: 1 only for x a hair below an integer, the same point as (cc + 1, 0)
-            cf[a] = cn[a] + cc;
-        }
+        for (int a = 0; a < 3; ++a) add_cells_q(cf[a], o[a].x, o[a].y, d.dh[a], d.dl[a], fold);
         return 0;
     }
-    add_dh(f, d.dh);
-    if (((unsigned)(g + 1) & 3u) == 0u) carry(cf, f);
+    float2 Q[3], U[3];
+    drift_quanta(d, Q, U);
+    drift_enter(o, U);
+    add_quanta(o, Q);
+    if (((unsigned)(g + 1) & kCarryMask) == 0u) carry(cf, o, U);
+    normalise(cf, o);
     // the next steps' pre-test, decided now from the normalised position
-    add_dh(fn, d.dh);
-    return quiet_steps(P, cn, fn, d.dh);
+    const float fnext[3] = {o[0].x, o[1].x, o[2].x};
+    return quiet_steps(P, cf, fnext, Q);
 }
 
 template <int ALG, bool RF, int L>
-__device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float vh[3], float vl[3], Drift& d,
-                                           int64_t g) {
+__device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], float fl[3], float vh[3], float vl[3],
+                                           Drift& d, int64_t g) {
     const TrackMixDev& P = *c.P;
     F3 v = f3(vh[0], vh[1], vh[2]);
     if constexpr (ALG == PPT_ALG_VAY_REL) {
         F3 E, B;
-        fields_mixed<RF, L>(c, cell, f, g, 0.0, E, B);
+        fields_mixed<RF, L>(c, cell, f, fl, g, 0.0, E, B);
         F3 vn = vay_rel_f(v, E, B, P.qm, P.dtf);
         // increment relative to the float32 head keeps the low part's bits
         vel_add(vh, vl, vn - v);
-        advance(P, cell, f, vh, vl);
+        advance(P, cell, f, fl, vh, vl);
     } else {  // RK4 / RK4_REL (pusher.py:803-892), stage times t, t+h, t+h, t+dt
         constexpr bool REL = ALG == PPT_ALG_RK4_REL;
         const float dt = P.dtf, h = 0.5f * dt;
         F3 E, B;
         int sc[3];
         float sf[3];
-        fields_mixed<RF, L>(c, cell, f, g, 0.0, E, B);
+        const float sl[3] = {0.0f, 0.0f, 0.0f};   // stage positions: high words only
+        fields_mixed<RF, L>(c, cell, f, fl, g, 0.0, E, B);
         F3 k1 = REL ? rk4_rel_deriv_f(v, E, B, P.qm) : lorentz_f(v, E, B, P.qm);
         F3 v2 = v + h * k1;
         offset_point(P, cell, f, h * v, sc, sf);
-        fields_mixed<RF, L>(c, sc, sf, g, 0.5 * P.dt, E, B);
+        fields_mixed<RF, L>(c, sc, sf, sl, g, 0.5 * P.dt, E, B);
         F3 k2 = REL ? rk4_rel_deriv_f(v2, E, B, P.qm) : lorentz_f(v2, E, B, P.qm);
         F3 v3_ = v + h * k2;
         offset_point(P, cell, f, h * v2, sc, sf);
-        fields_mixed<RF, L>(c, sc, sf, g, 0.5 * P.dt, E, B);
+        fields_mixed<RF, L>(c, sc, sf, sl, g, 0.5 * P.dt, E, B);
         F3 k3 = REL ? rk4_rel_deriv_f(v3_, E, B, P.qm) : lorentz_f(v3_, E, B, P.qm);
         F3 v4 = v + dt * k3;
         offset_point(P, cell, f, dt * v3_, sc, sf);
-        fields_mixed<RF, L>(c, sc, sf, g, P.dt, E, B);
+        fields_mixed<RF, L>(c, sc, sf, sl, g, P.dt, E, B);
         F3 k4 = REL ? rk4_rel_deriv_f(v4, E, B, P.qm) : lorentz_f(v4, E, B, P.qm);
         // r_new - r = dt v + dt^2/6 (k1 + k2 + k3); v_new - v = dt/6 (k1 + 2k2 + 2k3 + k4)
         const float s6 = dt * (1.0f / 6.0f);
         F3 dr = (dt * s6) * (k1 + k2 + k3);
         F3 dv = s6 * (k1 + 2.0f * k2 + 2.0f * k3 + k4);
         const float drv[3] = {dr.x, dr.y, dr.z};
-        // position: the dt v part in float-float, the stage correction in float32
-        advance(P, cell, f, vh, vl);
+        // position: the dt v part in float-float, the stage correction (in
+        // cells) added with it into the float-float offset
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float g = fmaf(drv[a], P.inv_d[a], f[a]);
-            float cc = floorf(g);
-            f[a] = g - cc;
-            cell[a] += (int)cc;
-            if (f[a] >= 1.0f) { f[a] -= 1.0f; cell[a] += 1; }
-        }
+        for (int a = 0; a < 3; ++a)
+            advance_axis(cell[a], f[a], fl[a], vh[a], vl[a], P.kh[a], P.kl[a], drv[a] * P.inv_d[a]);
         vel_add(vh, vl, dv);
         if (REL) {
             F3 vn = f3(vh[0], vh[1], vh[2]);
@@ -642,24 +1022,44 @@ __device__ __forceinline__ void mixed_step(MixCtx& c, int cell[3], float f[3], f
     }
 }
 
-// Snapshot row: x = lo + (cell + f) d and v = vh + vl, formed in float64
-// (output formatting only).
+// Snapshot row: x = lo + (cell + f + fl) d and v = vh + vl (u / gamma(u)
+// for the u state), formed in float64 (output formatting only).
 __device__ __forceinline__ void write_mixed_row(const TrackMixDev& P, int64_t rec, int64_t row, const int cell[3],
-                                                const float f[3], const float vh[3], const float vl[3],
-                                                bool r_too) {
+                                                const float f[3], const float fl[3], const float vh[3],
+                                                const float vl[3], bool r_too, bool u_state = false) {
     const int64_t o = (rec * P.n + row) * 3;
+    double w[3] = {(double)vh[0] + (double)vl[0], (double)vh[1] + (double)vl[1], (double)vh[2] + (double)vl[2]};
+    if (u_state) {
+        const double ig = 1.0 / sqrt(1.0 + (w[0] * w[0] + w[1] * w[1] + w[2] * w[2]) / (kClight * kClight));
+        w[0] *= ig;
+        w[1] *= ig;
+        w[2] *= ig;
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        if (r_too) P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + (double)f[a]) * P.G.d[a];
-        P.v_hist[o + a] = (double)vh[a] + (double)vl[a];
+        if (r_too) P.r_hist[o + a] = P.G.lo[a] + ((double)cell[a] + ((double)f[a] + (double)fl[a])) * P.G.d[a];
+        P.v_hist[o + a] = w[a];
     }
 }
 
+__host__ __device__ constexpr bool alg_u_family(int a) { return a == PPT_ALG_BORIS_REL || a == PPT_ALG_VAY; }
+
+// Half step (+-dt/2 through hq = +-hqdt/2) of the u-state pushers: the
+// staggering of the Boris family (the float64 form's half_kick).
+template <int ALG, int L>
+__device__ __forceinline__ void u_half_kick(float vh[3], float vl[3], F3 E, F3 B, float hq, float ws) {
+    float du[3], corr[3];
+    if constexpr (ALG == PPT_ALG_BORIS_REL) boris_rel_du<e_bits(L), b_bits(L)>(vh, E, B, hq, ws, du, corr);
+    else vay_du<e_bits(L), b_bits(L)>(vh, E, B, hq, ws, du, corr);
+    vel_add_corr(vh, vl, du, corr);
+    vel_renorm<7>(vh, vl);
+}
+
 // float64 position of (cell + offset) on the tracking grid (the snapshot rows' formula)
-__device__ __forceinline__ V3 mixed_position(const TrackMixDev& P, const float cf[3], const float f[3]) {
-    return v3(P.G.lo[0] + ((double)cf[0] + (double)f[0]) * P.G.d[0],
-              P.G.lo[1] + ((double)cf[1] + (double)f[1]) * P.G.d[1],
-              P.G.lo[2] + ((double)cf[2] + (double)f[2]) * P.G.d[2]);
+__device__ __forceinline__ V3 mixed_position(const TrackMixDev& P, const float cf[3], const float2 o[3]) {
+    return v3(P.G.lo[0] + ((double)cf[0] + ((double)o[0].x + (double)o[0].y)) * P.G.d[0],
+              P.G.lo[1] + ((double)cf[1] + ((double)o[1].x + (double)o[1].y)) * P.G.d[1],
+              P.G.lo[2] + ((double)cf[2] + ((double)o[2].x + (double)o[2].y)) * P.G.d[2]);
 }
 
 // COLL (Boris only): each step's segment, from the float64 positions before
@@ -676,40 +1076,49 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
         bool stopped = false;
         unsigned steps_done = (unsigned)P.nsteps;
         int cell[3];
-        float f[3], vh[3], vl[3];
+        float f[3], fl[3], vh[3], vl[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             cell[a] = P.ci[a * n + s];
             f[a] = P.fs[a * n + s];
             vh[a] = P.fs[(3 + a) * n + s];
             vl[a] = P.fs[(6 + a) * n + s];
+            fl[a] = P.fs[(9 + a) * n + s];
         }
         const int64_t row = P.order ? P.order[s] : s;
         if (RF) {
             c.phase = fma(P.omega, P.t0, P.rf_phase[s]);   // omega t0 + phi_i
             double sa, ca;
             sincos(c.phase, &sa, &ca);
-            c.c0 = (float)ca;
-            c.s0 = (float)sa;
+            const float2 cp = split_d(ca), sp = split_d(sa);
+            c.c0h = cp.x;
+            c.c0l = cp.y;
+            c.s0h = sp.x;
+            c.s0l = sp.y;
         }
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
                 F3 E, B;
-                if (fields_mixed<RF, L>(c, cell, f, P.step0, 0.0, E, B))
+                if (fields_mixed<RF, L>(c, cell, f, fl, P.step0, 0.0, E, B))
                     // Boris push with time step -dt/2 (pusher.py:947-958): half of hqdt
                     vel_add_boris<boris_bits(L)>(vh, vl, boris_dv<L>(f3(vh[0], vh[1], vh[2]), E, B, -0.5f * P.hqdt),
                                                  P.wscale);
+            } else if constexpr (alg_u_family(ALG)) {
+                F3 E, B;
+                if (fields_mixed<RF, L>(c, cell, f, fl, P.step0, 0.0, E, B)) u_half_kick<ALG, L>(vh, vl, E, B, -0.5f * P.hqdt, P.wscale);
             }
-            if (P.r_hist) write_mixed_row(P, 0, row, cell, f, vh, vl, true);
+            if (P.r_hist) write_mixed_row(P, 0, row, cell, f, fl, vh, vl, true, alg_u_family(ALG));
         }
         Drift d;
-        increment(P, vh, vl, d.dh, d.dl);
+        if constexpr (alg_u_family(ALG)) increment_u(P, vh, vl, d.dh, d.dl);
+        else increment(P, vh, vl, d.dh, d.dl);
         const int nsteps = (int)P.nsteps;
         const int rec_every = P.rec_every > 0x7fffffff ? 0x7fffffff : (int)P.rec_every;
         const int64_t until64 = P.rec_every - 1 - (P.step0 % P.rec_every);
         int until = until64 > 0x7fffffff ? 0x7fffffff : (int)until64;   // beyond this launch anyway
-        if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG) {
+        if constexpr (ALG == PPT_ALG_BORIS || ALG == PPT_ALG_LEAPFROG || alg_u_family(ALG)) {
             float cf[3] = {(float)cell[0], (float)cell[1], (float)cell[2]};
+            float2 o[3] = {make_float2(f[0], fl[0]), make_float2(f[1], fl[1]), make_float2(f[2], fl[2])};
             // record-free segments: the inner loop carries only its counter
             int k = 0;
             int quiet = 0;   // upcoming steps known to be field-free (quiet_steps)
@@ -721,10 +1130,10 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                     // one step at a time, each segment tested (no field-free runs)
                     int i = 0;
                     while (i < seg) {
-                        const V3 r0 = mixed_position(P, cf, f);
-                        family_step<ALG, RF, L>(c, cf, f, vh, vl, d, g0 + i);
+                        const V3 r0 = mixed_position(P, cf, o);
+                        family_step<ALG, RF, L>(c, cf, o, vh, vl, d, g0 + i);
                         ++i;
-                        if (segment_hits_surface(C->surf, r0, mixed_position(P, cf, f))) {
+                        if (segment_hits_surface(C->surf, r0, mixed_position(P, cf, o))) {
                             stopped = true;
                             break;
                         }
@@ -734,7 +1143,8 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                     if ((int64_t)i == to_rec) {
                         const int64_t rec = (P.step0 + k) / P.rec_every;
                         const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
-                        if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
+                        const float oh[3] = {o[0].x, o[1].x, o[2].x}, ol[3] = {o[0].y, o[1].y, o[2].y};
+                        if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, oh, ol, vh, vl, true, alg_u_family(ALG));
                         until = rec_every - 1;
                     } else {
                         until -= i;
@@ -748,11 +1158,13 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 for (int i = 0; i < seg;) {
                     if (quiet > 0) {
                         const int m = quiet < seg - i ? quiet : seg - i;
-                        drift_steps(cf, f, d.dh, g0 + i, m);
+                        float2 Q[3], U[3];
+                        drift_quanta(d, Q, U);
+                        drift_steps(cf, o, Q, U, g0 + i, m);
                         i += m;
                         quiet -= m;
                     } else {
-                        quiet = family_step<ALG, RF, L>(c, cf, f, vh, vl, d, g0 + i);
+                        quiet = family_step<ALG, RF, L>(c, cf, o, vh, vl, d, g0 + i);
                         ++i;
                     }
                 }
@@ -760,7 +1172,8 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                 if ((int64_t)seg == to_rec) {
                     const int64_t rec = (P.step0 + k) / P.rec_every;
                     const int ic[3] = {(int)cf[0], (int)cf[1], (int)cf[2]};
-                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, f, vh, vl, true);
+                    const float oh[3] = {o[0].x, o[1].x, o[2].x}, ol[3] = {o[0].y, o[1].y, o[2].y};
+                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, ic, oh, ol, vh, vl, true, alg_u_family(ALG));
                     until = rec_every - 1;
                 } else {
                     until -= seg;
@@ -768,13 +1181,17 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             }
             // the state keeps its (possibly uncarried) offset; exact anyway
 #pragma unroll
-            for (int a = 0; a < 3; ++a) cell[a] = (int)cf[a];
+            for (int a = 0; a < 3; ++a) {
+                cell[a] = (int)cf[a];
+                f[a] = o[a].x;
+                fl[a] = o[a].y;
+            }
         } else {
             for (int k = 0; k < nsteps; ++k) {
-                mixed_step<ALG, RF, L>(c, cell, f, vh, vl, d, P.step0 + k);
+                mixed_step<ALG, RF, L>(c, cell, f, fl, vh, vl, d, P.step0 + k);
                 if (until == 0) {
                     const int64_t rec = (P.step0 + k + 1) / P.rec_every;
-                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, vh, vl, true);
+                    if (P.r_hist && rec < P.n_rec) write_mixed_row(P, rec, row, cell, f, fl, vh, vl, true);
                     until = rec_every - 1;
                 } else {
                     --until;
@@ -792,11 +1209,24 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                     cn[a] = cell[a] + (int)cc;
                     fn[a] = f[a] - cc;
                 }
-                if (fields_mixed<RF, L>(c, cn, fn, P.nsteps_total, 0.0, E, B))
+                if (fields_mixed<RF, L>(c, cn, fn, fl, P.nsteps_total, 0.0, E, B))
                     // Boris push with time step +dt/2 (pusher.py:993-1007)
                     vel_add_boris<boris_bits(L)>(vh, vl, boris_dv<L>(f3(vh[0], vh[1], vh[2]), E, B, 0.5f * P.hqdt),
                                                  P.wscale);
-                if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, vh, vl, false);
+                if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, fl, vh, vl, false);
+            } else if constexpr (alg_u_family(ALG)) {
+                F3 E, B;
+                int cn[3];
+                float fn[3];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float cc = floorf(f[a]);
+                    cn[a] = cell[a] + (int)cc;
+                    fn[a] = f[a] - cc;
+                }
+                if (fields_mixed<RF, L>(c, cn, fn, fl, P.nsteps_total, 0.0, E, B))
+                    u_half_kick<ALG, L>(vh, vl, E, B, 0.5f * P.hqdt, P.wscale);
+                if (P.v_hist) write_mixed_row(P, P.n_rec - 1, row, cell, f, fl, vh, vl, false, true);
             }
         }
 #pragma unroll
@@ -805,6 +1235,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             P.fs[a * n + s] = f[a];
             P.fs[(3 + a) * n + s] = vh[a];
             P.fs[(6 + a) * n + s] = vl[a];
+            P.fs[(9 + a) * n + s] = fl[a];
         }
         if (P.status) {
             float sum = f[0] + f[1] + f[2] + vh[0] + vh[1] + vh[2];
@@ -823,9 +1254,9 @@ template <int ALG, bool RF, int L>
 __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, nullptr, 0};
+    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
     if constexpr (RF) {
-        extern __shared__ float2 rf_tab[];
+        extern __shared__ float4 rf_tab[];
         if (P.rf_tab_n > 0) {
             build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
             c.tab = rf_tab;
@@ -842,9 +1273,9 @@ __global__ void __launch_bounds__(128) track_mixed_coll_kernel(const __grid_cons
                                                                const __grid_constant__ CollDev C) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, nullptr, 0};
+    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
     if constexpr (RF) {
-        extern __shared__ float2 rf_tab[];
+        extern __shared__ float4 rf_tab[];
         if (P.rf_tab_n > 0) {
             build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
             c.tab = rf_tab;
@@ -886,10 +1317,10 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
         __syncthreads();
         if (sP.flags >= 0) {
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
-            MixCtx c{&sP, 0.0, 0u, 0.0f, 0.0f, nullptr, 0};
+            MixCtx c{&sP, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
             if constexpr (RF) {
                 // this job's step window, when the launch reserved a table for it
-                extern __shared__ float2 rf_tab[];
+                extern __shared__ float4 rf_tab[];
                 const int nt = (int)sP.nsteps + 1;
                 if (Q.chunk + 1 <= kRfTable && nt <= kRfTable) {
                     build_rf_table(rf_tab, sP.step0, nt, sP.wdt);
@@ -914,11 +1345,11 @@ static cudaError_t launch_mixed_layout(const TrackMixDev* P, const JobQueueDev* 
     if (P) {
         const int block = pick_block(P->n);
         const int g = grid_for(P->n, block);
-        const size_t smem = (size_t)P->rf_tab_n * sizeof(float2);
+        const size_t smem = (size_t)P->rf_tab_n * sizeof(float4);
         if (rf && kE) track_mixed_kernel<ALG, kE, L><<<g, block, smem, s>>>(*P);
         else track_mixed_kernel<ALG, false, L><<<g, block, 0, s>>>(*P);
     } else {
-        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(float2) : 0;
+        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(float4) : 0;
         if (rf && kE) track_mixed_jobs_kernel<ALG, kE, L><<<grid, kJobBlock, smem, s>>>(*Q);
         else track_mixed_jobs_kernel<ALG, false, L><<<grid, kJobBlock, 0, s>>>(*Q);
     }
@@ -947,9 +1378,11 @@ static int launch_mixed(const TrackMixDev* P, const JobQueueDev* Q, int algorith
         case PPT_ALG_RK4: e = launch_mixed_alg<PPT_ALG_RK4>(P, Q, layout, rf, grid, s); break;
         case PPT_ALG_VAY_REL: e = launch_mixed_alg<PPT_ALG_VAY_REL>(P, Q, layout, rf, grid, s); break;
         case PPT_ALG_RK4_REL: e = launch_mixed_alg<PPT_ALG_RK4_REL>(P, Q, layout, rf, grid, s); break;
+        case PPT_ALG_BORIS_REL: e = launch_mixed_alg<PPT_ALG_BORIS_REL>(P, Q, layout, rf, grid, s); break;
+        case PPT_ALG_VAY: e = launch_mixed_alg<PPT_ALG_VAY>(P, Q, layout, rf, grid, s); break;
         default:
-            return fail(PPT_ERR_UNSUPPORTED,
-                        "the mixed form covers leapfrog, boris, rk4, vay_rel and rk4_rel; use precision 'fp64'");
+            return fail(PPT_ERR_UNSUPPORTED, "the mixed form covers leapfrog, boris, rk4, vay_rel, rk4_rel, boris_rel "
+                                             "and vay; use precision 'fp64'");
     }
     if (e != cudaSuccess) return cuda_fail(e, what);
     return PPT_OK;
@@ -968,7 +1401,7 @@ static cudaError_t launch_coll_layout(const TrackMixDev& P, const CollDev& C, bo
     constexpr bool kE = layout_has_e(L);
     const int block = pick_block(P.n);
     const int g = grid_for(P.n, block);
-    if (rf && kE) track_mixed_coll_kernel<kE, L><<<g, block, (size_t)P.rf_tab_n * sizeof(float2), s>>>(P, C);
+    if (rf && kE) track_mixed_coll_kernel<kE, L><<<g, block, (size_t)P.rf_tab_n * sizeof(float4), s>>>(P, C);
     else track_mixed_coll_kernel<false, L><<<g, block, 0, s>>>(P, C);
     return cudaGetLastError();
 }
@@ -1026,9 +1459,9 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
     P->qm = (float)a->q_over_m;
     P->hqdt = (float)(0.5 * a->q_over_m * a->dt);
     P->wscale = 0.0f;
-    if (st->algorithm == PPT_ALG_BORIS) {
-        // Boris increments scaled by (1 + wscale): hqdt (1 + wscale) is q/m
-        // dt/2 to float64 accuracy
+    if (st->algorithm == PPT_ALG_BORIS || alg_u_family(st->algorithm)) {
+        // Boris-family increments scaled by (1 + wscale): hqdt (1 + wscale) is
+        // q/m dt/2 to float64 accuracy
         const double exact = 0.5 * a->q_over_m * a->dt;
         const double ws = exact / (double)P->hqdt - 1.0;
         P->wscale = (float)ws;

@@ -29,6 +29,9 @@ struct TrackDev {
     unsigned long long* counters;
     SurfaceDev surf;    // electrode surface (n_tri = 0: none)
     uint8_t* active;    // row order; with a surface, 0 = stopped by it
+    const double* dt_rows;   // RK4 / rk4_rel: one dt per particle, row order (NULL: dt)
+    int32_t rf_tab_n;        // entries of the per-step RF table a launch builds (0: none)
+    int32_t pad_;
 };
 
 struct TrackMixDev {
@@ -94,6 +97,15 @@ struct JobQueueDev {
 
 constexpr int kJobBlock = 128;
 
+// The record layout a float64 launch is specialised on: one uniform-grid map
+// and no constant field parts; 0 otherwise (the run-time dispatch over any
+// number of maps).  Single tracks and serving jobs use the same rule, so a
+// job runs the same kernel code alone and in a serving mix.
+inline int f64_single_layout(const TrackDev& P) {
+    if (P.F.n_maps != 1 || P.F.e_const_nz || P.F.b_const_nz || !P.F.maps[0].all_uniform) return 0;
+    return P.F.maps[0].layout;
+}
+
 int mixed_grid(const FieldsDev& F, GridF* G);
 int check_state(const ppt_state* st);
 int launch_track_f64(const TrackDev& P, int algorithm, bool rf, bool surface, cudaStream_t s);
@@ -101,7 +113,7 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
                      TrackMixDev* P);
 int launch_track_mixed(const TrackMixDev& P, int algorithm, bool rf, cudaStream_t s);
 int launch_track_mixed_coll(const TrackMixDev& P, const CollDev& C, bool rf, cudaStream_t s);
-int launch_f64_jobs(const JobQueueDev& Q, int algorithm, bool rf, int grid, cudaStream_t s);
+int launch_f64_jobs(const JobQueueDev& Q, int algorithm, int layout, bool rf, int grid, cudaStream_t s);
 int launch_mixed_jobs(const JobQueueDev& Q, int algorithm, int layout, bool rf, int grid, cudaStream_t s);
 
 // Device helper shared by both job kernels: thread 0 takes the next item and

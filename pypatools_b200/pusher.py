@@ -25,6 +25,7 @@ cos(2 pi f t + phi_i)) and ``t0``.  ``electrode_assembly`` takes an
 All work runs in libppt.so kernels; there is no CPU fallback.
 """
 import math
+import mmap
 import warnings
 
 import numpy as np
@@ -34,7 +35,7 @@ from .device_fields import FieldCache
 
 REFERENCE_ALGORITHMS = ["leapfrog", "boris", "rk4", "yoshida", "vay_rel", "rk4_rel", "yoshida_rel"]
 EXTRA_ALGORITHMS = ["boris_rel", "vay"]
-MIXED_ALGORITHMS = ("leapfrog", "boris", "rk4", "vay_rel", "rk4_rel")
+MIXED_ALGORITHMS = ("leapfrog", "boris", "rk4", "vay_rel", "rk4_rel", "boris_rel", "vay")
 
 
 class RFModulation:
@@ -93,7 +94,7 @@ class DeviceTracker:
 
     def __init__(self, algorithm, q_over_m, dfields, n, nsteps_total, dt, rec_every=1, precision="fp64",
                  rf_omega=0.0, rf_phase=None, t0=0.0, record=True, stagger=True, counters=False,
-                 device=None, surface=None):
+                 device=None, surface=None, dt_rows=None):
         torch = _torch()
         self.torch = torch
         if algorithm not in _lib.ALG_IDS:
@@ -126,7 +127,7 @@ class DeviceTracker:
         else:
             self.f64 = None
             self.i32 = torch.empty(3 * n, dtype=torch.int32, device=dev)
-            self.f32 = torch.empty(9 * n, dtype=torch.float32, device=dev)
+            self.f32 = torch.empty(12 * n, dtype=torch.float32, device=dev)
         self.state = _lib.State(_lib.PREC_F64 if precision == "fp64" else _lib.PREC_MIXED,
                                 _lib.ALG_IDS[algorithm], n,
                                 self.f64.data_ptr() if self.f64 is not None else None,
@@ -161,6 +162,16 @@ class DeviceTracker:
             self.rf_phase = ph.to(dev).contiguous().clone()
         else:
             self.rf_phase = None
+        # one time step per particle (row order): the float64 RK4 pushers only,
+        # as in the reference's batch RK4 step (pusher.py:815-816)
+        self.dt_rows = None
+        if dt_rows is not None:
+            if precision != "fp64" or algorithm not in ("rk4", "rk4_rel"):
+                raise NotImplementedError("a per-particle dt runs in the float64 form of rk4 and rk4_rel")
+            d = torch.as_tensor(dt_rows, dtype=torch.float64)
+            if tuple(d.shape) != (n,):
+                raise ValueError(f"dt must be a scalar or ({n},), got {tuple(d.shape)}")
+            self.dt_rows = d.to(dev).contiguous().clone()
         self.order = None
         self.sort_scratch = None
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -208,6 +219,8 @@ class DeviceTracker:
         if self.surface is not None:
             a.surface = self.surface
             a.active = self.active.data_ptr()
+        if self.dt_rows is not None:
+            a.dt_rows = self.dt_rows.data_ptr()
         _lib.check(self.lib.ppt_track(self.state, self.dfields.fields, a, self._stream(stream)))
         if k > 0 or flags:
             self.launches += 1
@@ -327,21 +340,37 @@ class DeviceTracker:
         return {"map_hits": int(c[0]), "particle_steps": int(c[1])}
 
 
-class HostStager:
-    """Device -> numpy copies through a ring of pinned buffers.
+def host_array(shape, dtype=np.float64):
+    """A fresh numpy array for results the GPU fills, backed (from 64 MiB up)
+    by anonymous memory advised for transparent huge pages: writing tens of
+    GB into fresh 4 KiB pages is bound by page faults (27 GB/s measured with
+    24 threads on a B200 host), with huge pages the copies run at PCIe speed
+    (50 GB/s).  The array owns its mapping; it is released with the array."""
+    nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    if nbytes < (64 << 20) or not hasattr(mmap, "MADV_HUGEPAGE"):
+        return np.empty(shape, dtype)
+    m = mmap.mmap(-1, nbytes, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
+    try:
+        m.madvise(mmap.MADV_HUGEPAGE)
+    except OSError:
+        pass            # transparent huge pages off: plain pages, still correct
+    return np.frombuffer(m, dtype=dtype).reshape(shape)
 
-    Each piece (``chunk`` bytes at most) goes device -> pinned buffer on a copy
-    stream (PCIe at full speed, ~50 GB/s on B200 hosts), then a worker thread
-    copies it into the destination numpy array (numpy releases the GIL for
-    the copy, which also maps the fresh array's pages); the ring keeps
-    ``slots`` pieces in flight.  Pinning the destination instead costs about a
+
+class HostStager:
+    """Host <-> device copies through a ring of pinned buffers.
+
+    Device -> numpy: each piece (``chunk`` bytes at most) goes device -> pinned
+    buffer on a copy stream (PCIe at ~50 GB/s on B200 hosts), then a worker
+    thread copies it into the destination numpy array (numpy releases the GIL
+    for the copy); the ring keeps ``slots`` pieces in flight.  The
+    destinations of ``track_batch`` are fresh huge-page-advised arrays
+    (``host_array``), whose first touch keeps up with the link; with 4 KiB
+    pages it ran at half of it.  Pinning the destination instead costs about a
     second per 1.5 GB whenever the caller still holds earlier results, and a
-    device copy into pageable memory runs at ~2 GB/s.  Measured on the 1e7
-    proton x 41-record job (19.7 GB of histories): 0.70-0.73 s per call with
-    24 slots of 32 MB, kept or dropped results alike (6 x 128 MB: 1.05 s;
-    pinning the whole histories: 0.70 s while torch's pinned cache can reuse a
-    dropped result, 14 s when the caller keeps them; touching the fresh
-    pages from a second thread group first: 0.79 s)."""
+    device copy into pageable memory runs at ~2 GB/s.  numpy -> device
+    (``upload``): worker threads copy the pieces into the pinned buffers and
+    enqueue their host-to-device copies."""
 
     _by_device = {}
 
@@ -398,6 +427,39 @@ class HostStager:
     def _land(self, k, db, a, b):
         self.events[k].synchronize()
         np.copyto(db[a:b], self.views[k][:b - a])
+
+    def upload(self, src, dst):
+        """Copy the contiguous numpy array ``src`` into the contiguous device
+        tensor ``dst`` (same bytes) through the ring: worker threads copy the
+        pieces into the pinned buffers and enqueue each piece's host-to-device
+        copy on the copy stream.  Returns an event recorded after the last
+        piece; the caller's stream waits on it before reading ``dst``."""
+        torch = self.torch
+        sb = src.reshape(-1).view(np.uint8)
+        db = dst.reshape(-1).view(torch.uint8)
+        with self.lock:
+            staged = []
+            for a in range(0, sb.size, self.chunk):
+                b = min(a + self.chunk, sb.size)
+                k = self.next
+                self.next = (k + 1) % len(self.buffers)
+                if self.pending[k] is not None:
+                    self.pending[k].result()      # the slot's previous piece has landed or left
+                self.events[k].synchronize()      # and its last copy is done
+                self.pending[k] = self.pool.submit(self._stage, k, sb, db, a, b)
+                staged.append(self.pending[k])
+            for f in staged:
+                f.result()
+            ev = torch.cuda.Event()
+            ev.record(self.stream)
+        return ev
+
+    def _stage(self, k, sb, db, a, b):
+        torch = self.torch
+        np.copyto(self.views[k][:b - a], sb[a:b])
+        with torch.cuda.device(self.device), torch.cuda.stream(self.stream):
+            db[a:b].copy_(self.buffers[k][:b - a], non_blocking=True)
+            self.events[k].record(self.stream)
 
     def finish(self):
         with self.lock:
@@ -474,6 +536,19 @@ class PusherGPU:
             raise ValueError(f"{name} must have shape (M, 3), got {a.shape}")
         return a
 
+    def _time_step(self, dt, m):
+        """(scalar dt, per-particle dt or None).  The reference's batch RK4
+        step takes an array dt, one value per particle (pusher.py:815-816);
+        its other pushers take a float."""
+        if np.isscalar(dt) or np.ndim(dt) == 0:
+            return float(dt), None
+        if self.algorithm not in ("rk4", "rk4_rel") or self.precision != "fp64":
+            raise TypeError("dt must be a scalar (an array dt is taken by the float64 rk4 and rk4_rel only)")
+        d = np.ascontiguousarray(np.asarray(dt, dtype=np.float64))
+        if d.shape != (m,):
+            raise ValueError(f"dt must be a scalar or have shape ({m},), got {d.shape}")
+        return (float(d[0]) if m else 0.0), d
+
     def _upload(self, a, device):
         torch = _torch()
         t = torch.from_numpy(a)
@@ -484,20 +559,20 @@ class PusherGPU:
     # -- batch API -----------------------------------------------------------
     def push_batch(self, r_array, v_array, efield, bfield, dt):
         """One step for M particles (pusher.py:699-801): no half-step
-        staggering, exactly the reference's push_batch."""
-        if not np.isscalar(dt):
-            raise TypeError("dt must be a scalar on the GPU path")
+        staggering, exactly the reference's push_batch.  ``dt`` may be an (M,)
+        array for rk4 / rk4_rel in the float64 form, as in the reference."""
         r = self._as_rows(r_array, "r_array")
         v = self._as_rows(v_array, "v_array")
         if r.shape != v.shape:
             raise ValueError("r_array and v_array must have the same shape")
         m = r.shape[0]
+        dt, dt_rows = self._time_step(dt, m)
         if m == 0:
             return r.copy(), v.copy()
         torch = _torch()
         df = self._device_fields(efield, bfield)
         tr = DeviceTracker(self.algorithm, self.q_over_m, df, m, 1, dt, 1, self.precision, record=False,
-                           stagger=False, device=self.device)
+                           stagger=False, device=self.device, dt_rows=dt_rows)
         d_r, d_v = self._upload(r, df.device), self._upload(v, df.device)
         with torch.cuda.device(df.device):
             tr.load(d_r, d_v)
@@ -511,9 +586,9 @@ class PusherGPU:
         (r_hist (n_rec, M, 3), v_hist, active (M,)) with
         n_rec = nsteps // rec_every_n_steps + 1.  With an electrode assembly,
         a particle whose step meets it stops after that step (its later rows
-        stay NaN, no closing half step) and is False in ``active``."""
-        if not np.isscalar(dt):
-            raise TypeError("dt must be a scalar on the GPU path")
+        stay NaN, no closing half step) and is False in ``active``.  ``dt``
+        may be an (M,) array for rk4 / rk4_rel in the float64 form, as in
+        the reference."""
         nsteps = int(nsteps)
         rec = int(rec_every_n_steps)
         if nsteps < 0:
@@ -525,6 +600,7 @@ class PusherGPU:
         if r0.shape != v0.shape:
             raise ValueError("r0_array and v0_array must have the same shape")
         m = r0.shape[0]
+        dt, dt_rows = self._time_step(dt, m)
         n_rec = nsteps // rec + 1
         torch = _torch()
         if m == 0:
@@ -534,15 +610,26 @@ class PusherGPU:
                         np.ones(0, dtype=bool))
             return empty, empty.copy(), np.ones(0, dtype=bool)
         df = self._device_fields(efield, bfield)
+        stager = HostStager.for_device(df.device)
+        uploads = []
+
+        def upload(a):
+            t = torch.empty(a.shape, dtype=torch.float64, device=df.device)
+            uploads.append(stager.upload(np.ascontiguousarray(a, dtype=np.float64), t))
+            return t
+
         rf_omega, rf_phase = 0.0, None
         if rf is not None:
             rf_omega = rf.omega
-            rf_phase = np.array(np.broadcast_to(np.asarray(rf.phase, dtype=np.float64), (m,)))
-            rf_phase = torch.from_numpy(rf_phase)
+            rf_phase = upload(np.broadcast_to(np.asarray(rf.phase, dtype=np.float64), (m,)))
+        d_r0, d_v0 = upload(r0), upload(v0)
+        with torch.cuda.device(df.device):
+            for ev in uploads:                 # the tracker reads them on this stream
+                torch.cuda.current_stream().wait_event(ev)
         surface = self.surface if _collide else None
         tr = DeviceTracker(self.algorithm, self.q_over_m, df, m, nsteps, dt, rec, self.precision,
                            rf_omega=rf_omega, rf_phase=rf_phase, t0=t0, record=True, device=self.device,
-                           surface=surface)
+                           surface=surface, dt_rows=dt_rows)
         self.last_tracker = tr
         chunk = self.steps_per_launch or default_steps_per_launch(m, nsteps)
         sort_every = self._sort_interval(m)
@@ -555,9 +642,8 @@ class PusherGPU:
                 # launches run: finished rows go through a small ring of
                 # pinned buffers (HostStager) instead of pinning the whole
                 # histories, which costs seconds per call for large bunches.
-                h_r = np.empty((n_rec, m, 3))
-                h_v = np.empty((n_rec, m, 3))
-                stager = HostStager.for_device(df.device)
+                h_r = host_array((n_rec, m, 3))
+                h_v = host_array((n_rec, m, 3))
                 compute = torch.cuda.current_stream()
                 copied = 0
 
@@ -570,7 +656,7 @@ class PusherGPU:
                     stager.copy(tr.r_hist[copied:upto], h_r[copied:upto], ev)
                     stager.copy(tr.v_hist[copied:upto], h_v[copied:upto], ev)
                     copied = upto
-            tr.load(self._upload(r0, df.device), self._upload(v0, df.device))
+            tr.load(d_r0, d_v0)
 
             def after_launch(done):
                 if verbose:

@@ -68,7 +68,7 @@ class TrackingJob:
         self._fields = None
 
     def device_bytes(self):
-        state = 48 * self.n                      # float64 state, or mixed (12 B cells + 36 B floats)
+        state = 60 * self.n                      # mixed (12 B cells + 48 B floats); float64 48 B
         hist = 2 * self.n_rec * self.n * 24
         phase = 8 * self.n if self.rf is not None else 0
         return state + hist + phase + 4096

@@ -5,11 +5,11 @@ golden vectors or tests for the pusher path, so parity is pinned by running
 its own ``Pusher.track_batch`` / ``Pusher.track`` / ``Field`` /
 ``ParticleDistribution`` code on seeded inputs and storing the results.
 
-Run from the repository root, with the reference checked out at
-``/root/reference`` (it is only needed to regenerate; the fixtures are
-committed):
+Run from the repository root, with PYPATOOLS_REFERENCE_SRC naming the
+reference checkout's ``src`` directory (it is only needed to regenerate; the
+fixtures are committed):
 
-    python tests/golden/make_golden.py
+    PYPATOOLS_REFERENCE_SRC=<checkout>/src python tests/golden/make_golden.py
 
 Import shims: ``pusher.py:33`` imports ``py_electrodes`` unconditionally and
 the package imports ``h5py`` and ``matplotlib`` at module level; none of them
@@ -26,7 +26,15 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE_SRC = "/root/reference/src"
+
+def reference_src():
+    """The reference checkout's ``src`` directory, from PYPATOOLS_REFERENCE_SRC."""
+    src = os.environ.get("PYPATOOLS_REFERENCE_SRC")
+    if not src or not (Path(src) / "PyPATools" / "pusher.py").is_file():
+        raise SystemExit("set PYPATOOLS_REFERENCE_SRC to the reference checkout's src directory "
+                         "(the one holding PyPATools/pusher.py)")
+    return src
+
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
 
@@ -48,7 +56,7 @@ def load_reference():
         sys.modules.setdefault(name, _Stub(name))
     cwd = os.getcwd()
     os.chdir(tempfile.mkdtemp(prefix="ppt_ref_"))
-    sys.path.insert(0, REFERENCE_SRC)
+    sys.path.insert(0, reference_src())
     try:
         from PyPATools import pusher, field, species, particles
     finally:

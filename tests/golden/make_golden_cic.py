@@ -13,7 +13,7 @@ the method is called on an instance whose grid attributes are set directly
 (the ones ``__init__`` sets at :178-185: extents, cell counts, spacings L/n).
 The module also cannot be imported without cupy (see ``main``).
 
-    python tests/golden/make_golden_cic.py
+    PYPATOOLS_REFERENCE_SRC=<checkout>/src python tests/golden/make_golden_cic.py
 """
 import sys
 import types

@@ -12,7 +12,7 @@ values, which ``NumbaInterpolator.__call__`` (interpolators.py:357-364) reads
 as ONE point of dimension M and rejects for M > 1 ("Points have dimension M,
 expected 1").  The fixture records that failure too.
 
-    python tests/golden/make_golden_fields12.py
+    PYPATOOLS_REFERENCE_SRC=<checkout>/src python tests/golden/make_golden_fields12.py
 """
 import sys
 from pathlib import Path

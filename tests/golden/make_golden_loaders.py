@@ -3,7 +3,7 @@ field-map loaders (src/PyPATools/field_src/field_loaders.py) on the synthetic
 files of loader_files.write_cases, and its Field.from_file (field.py:284-343)
 on each of them.
 
-    python tests/golden/make_golden_loaders.py
+    PYPATOOLS_REFERENCE_SRC=<checkout>/src python tests/golden/make_golden_loaders.py
 """
 import contextlib
 import io

@@ -12,7 +12,7 @@ potential.  For conductor cells, its classification (``_classify_cells``,
 followed by the assembly with Shortley-Weller rows.  The module needs inert stand-ins for cupy and pyamg to import
 (see make_golden_cic.py).
 
-    python tests/golden/make_golden_poisson.py
+    PYPATOOLS_REFERENCE_SRC=<checkout>/src python tests/golden/make_golden_poisson.py
 """
 import contextlib
 import io

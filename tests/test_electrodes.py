@@ -219,3 +219,63 @@ def test_gpu_mixed_boris_with_surface_vs_float64(cuda):
                         steps_per_launch=7).track_batch(wl.r0, wl.v0, e, b, 600, wl.dt, 50)
     for a, c in zip(out["mixed"], chunked):
         np.testing.assert_array_equal(a, c)
+
+
+def _mesh_grid(vertices, n_tri):
+    """The cell grid the library lays over a mesh (surface.cu, grid_for_mesh):
+    origin and cell size per axis."""
+    lo_in, hi_in = vertices.min(axis=0), vertices.max(axis=0)
+    big = float(np.max(hi_in - lo_in))
+    pad = max(big * 1e-9, 1e-30)
+    lo = lo_in - pad
+    ext = (hi_in + pad) - lo
+    side = np.cbrt(np.prod(ext) / max(1.0, 2.0 * n_tri))
+    dims = np.clip(np.ceil(ext / side), 1, 256)
+    return lo, ext / dims, dims.astype(int)
+
+
+@pytest.mark.gpu
+def test_gpu_triangles_on_cell_faces_match_oracle_bitwise(cuda):
+    """The mesh is binned into cells; the segment test works on v0 and the
+    rounded edge vectors, whose hits can lie an ulp outside the vertices' box.
+    Triangles with vertices exactly on cell faces (tilted, so the test's
+    arithmetic rounds) and short segments starting or ending on those faces
+    and a few ulps around them: the GPU's decisions must equal the oracle's,
+    which tests every triangle."""
+    rng = np.random.default_rng(17)
+    # a frame of 8 points fixes the mesh box, then 400 tilted triangles inside it
+    frame = np.array([[x, y, z] for x in (0.0, 1.0) for y in (0.0, 1.0) for z in (0.0, 1.0)])
+    n_tri = 402
+    lo, h, dims = _mesh_grid(frame, n_tri)
+    faces = [lo[a] + h[a] * np.arange(1, dims[a]) for a in range(3)]
+    tris, verts = [], [frame]
+    base = len(frame)
+    for t in range(n_tri - 2):
+        a = t % 3
+        f = rng.choice(faces[a])
+        v = rng.uniform(0.05, 0.95, (3, 3))
+        v[:, a] = f + rng.normal(0, 0.3, 3) * h[a]
+        v[rng.integers(0, 3), a] = f                            # one vertex exactly on the face
+        verts.append(v)
+        tris.append([base, base + 1, base + 2])
+        base += 3
+    tris.append([0, 1, 3])
+    tris.append([4, 5, 7])
+    vertices = np.concatenate(verts)
+    triangles = np.array(tris, dtype=np.int64)
+    s = ElectrodeSurface(vertices, triangles)
+    assert tuple(s.info()["cells"]) == tuple(dims)
+    m = 60000
+    a = rng.integers(0, 3, m)
+    p0 = rng.uniform(0.05, 0.95, (m, 3))
+    f = np.array([rng.choice(faces[k]) for k in a])
+    ulps = rng.integers(-3, 4, m).astype(float)
+    p0[np.arange(m), a] = f + ulps * np.spacing(f)
+    step = rng.normal(0, 1, (m, 3)) * 0.3 * h[None, :]
+    back = rng.uniform(size=m) < 0.5                           # half of them end on the face instead
+    p1 = p0 + step
+    p0[back], p1[back] = p1[back].copy(), p0[back].copy()
+    got = s.segment_intersects_surface(p0, p1)["hit_mask"]
+    ref = orc.segments_hit(p0, p1, vertices, triangles)
+    np.testing.assert_array_equal(got, ref)
+    assert ref.sum() > 1000

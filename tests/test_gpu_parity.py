@@ -142,3 +142,50 @@ def test_u_state_algorithms_vs_oracle(cuda, alg):
     ro, vo, _ = orc.track_batch(alg, wl.species.q_over_m, wl.r0, wl.v0, oe, ob, wl.nsteps, wl.dt, 500)
     assert rel_pos_err(rh, ro, half_width(wl)) < TOL
     assert rel_vel_err(vh, vo) < TOL
+
+
+@pytest.mark.parametrize("tag", ["quad", "radial"])
+@pytest.mark.parametrize("alg", ["rk4", "rk4_rel"])
+def test_rk4_per_particle_dt(cuda, tag, alg):
+    """One dt per particle, as the reference's batch RK4 step takes it
+    (pusher.py:815-816): track_batch and push_batch against the reference's
+    own outputs (tests/golden/dt_golden.npz), cell-sorted or not."""
+    from pathlib import Path
+    with np.load(Path(__file__).resolve().parent / "golden" / "dt_golden.npz") as d:
+        gold = {k: d[k] for k in d.files}
+    if tag == "quad":
+        wl = workloads.quad_solenoid_protons(n=96, nsteps=400, seed=21)
+    else:
+        wl = workloads.radial_e_solenoid_electrons(n=64, nsteps=800, seed=22)
+    e, b = gpu_fields(wl)
+    dt = gold[f"{tag}/dt"]
+    steps, rec = int(gold[f"{tag}/nsteps"]), int(gold[f"{tag}/rec"])
+    for sort_every in (0, 50):
+        p = PusherGPU(wl.species, alg, sort_every=sort_every, steps_per_launch=70)
+        rh, vh, _ = p.track_batch(wl.r0, wl.v0, e, b, steps, dt, rec)
+        assert rel_pos_err(rh, gold[f"{tag}/{alg}/r_hist"], half_width(wl)) < TOL
+        assert rel_vel_err(vh, gold[f"{tag}/{alg}/v_hist"]) < TOL
+    rn, vn = PusherGPU(wl.species, alg).push_batch(wl.r0, wl.v0, e, b, dt)
+    np.testing.assert_allclose(rn, gold[f"{tag}/{alg}/push_r"], rtol=1e-13, atol=0)
+    np.testing.assert_allclose(vn, gold[f"{tag}/{alg}/push_v"], rtol=1e-13, atol=0)
+
+
+def test_sector_ring_fp64_vs_c_oracle(cuda):
+    """The large-scale configuration's map, 512^3 float32 Bz over a 1 m cube
+    (the one-component record layout, float64 on the device, 1.1 GB): 1000
+    protons of its bunch for 2000 steps (about three turns), the float64 form
+    against the C oracle at 1e-10; the mixed form's error is reported."""
+    from oracle import cpu_baseline
+    wl = workloads.sector_ring_protons(n=1000, nsteps=2000, rec_every=500)
+    e, b = gpu_fields(wl)
+    omap, keep = cpu_baseline.make_map(wl.grid, wl.e_values, wl.b_values)
+    ro, vo = cpu_baseline.track("boris", wl.r0, wl.v0, omap, wl.nsteps, wl.dt, wl.species.q_over_m, wl.rec_every)
+    del keep
+    rh, vh, _ = PusherGPU(wl.species, "boris").track_batch(wl.r0, wl.v0, e, b, wl.nsteps, wl.dt, wl.rec_every)
+    assert rel_pos_err(rh, ro, half_width(wl)) < TOL
+    assert rel_vel_err(vh, vo) < TOL
+    rm, vm, _ = PusherGPU(wl.species, "boris", precision="mixed").track_batch(wl.r0, wl.v0, e, b, wl.nsteps,
+                                                                               wl.dt, wl.rec_every)
+    print(f"sector ring 1000 x 2000, mixed vs C oracle: pos {rel_pos_err(rm, ro, half_width(wl)):.3e} "
+          f"vel {rel_vel_err(vm, vo):.3e}")
+    assert rel_pos_err(rm, ro, half_width(wl)) < 1e-5

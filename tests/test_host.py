@@ -28,7 +28,7 @@ def test_library_exports_every_header_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(_lib.SIGNATURES)
-    assert lib.ppt_abi_version() == 2
+    assert lib.ppt_abi_version() == _lib.ABI_VERSION == 3
 
 
 def test_struct_layouts_match_header():
@@ -36,7 +36,7 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.GridDesc) == 48
     assert ctypes.sizeof(_lib.Fields) == 4 * 8 + 8 + 48
     assert ctypes.sizeof(_lib.State) == 40
-    assert ctypes.sizeof(_lib.TrackArgs) == 4 * 8 + 8 + 4 * 8 + 8 * 8
+    assert ctypes.sizeof(_lib.TrackArgs) == 4 * 8 + 8 + 4 * 8 + 9 * 8
 
 
 def test_capi_argument_errors_without_gpu():
@@ -177,6 +177,23 @@ def test_pusher_constructor_mirrors_reference():
         PusherGPU(ion, "boris", electrode_assembly=object())
     p.change_algorithm("boris")
     assert p.algorithm == "boris" and "PusherGPU(ion=proton" in repr(p)
+
+
+def test_array_dt_only_where_the_reference_takes_one():
+    """An (M,) dt array goes to the float64 rk4 / rk4_rel only (the
+    reference's batch RK4 step, pusher.py:815-816); it is checked on the host
+    before anything is uploaded."""
+    ion = IonSpecies("proton")
+    r = np.zeros((4, 3))
+    dts = np.full(4, 1e-11)
+    with pytest.raises(TypeError, match="dt must be a scalar"):
+        PusherGPU(ion, "boris").track_batch(r, r, None, None, 3, dts)
+    with pytest.raises(TypeError, match="dt must be a scalar"):
+        PusherGPU(ion, "rk4", precision="mixed").push_batch(r, r, None, None, dts)
+    with pytest.raises(ValueError, match=r"shape \(4,\)"):
+        PusherGPU(ion, "rk4").track_batch(r, r, None, None, 3, np.full(5, 1e-11))
+    assert PusherGPU(ion, "rk4_rel")._time_step(dts, 4)[1] is not None
+    assert PusherGPU(ion, "rk4_rel")._time_step(np.float64(1e-11), 4) == (1e-11, None)
 
 
 def test_state_rows_are_checked_before_a_launch():

@@ -132,3 +132,50 @@ def test_oracle_bunch_moments(golden):
                                rtol=1e-12)
     np.testing.assert_allclose(m["ekin_mean"], golden["pd/ekin_mean"], rtol=1e-12)
     np.testing.assert_allclose(m["ekin_std"], golden["pd/ekin_std"], rtol=1e-9)
+
+
+DT_GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "dt_golden.npz"
+
+
+@pytest.fixture(scope="module")
+def dt_golden():
+    with np.load(DT_GOLDEN) as d:
+        return {k: d[k] for k in d.files}
+
+
+def _dt_workload(tag):
+    if tag == "quad":
+        return workloads.quad_solenoid_protons(n=96, nsteps=400, seed=21)
+    return workloads.radial_e_solenoid_electrons(n=64, nsteps=800, seed=22)
+
+
+@pytest.mark.parametrize("tag", ["quad", "radial"])
+@pytest.mark.parametrize("alg", ["rk4", "rk4_rel"])
+def test_oracle_rk4_per_particle_dt(dt_golden, tag, alg):
+    """The reference's batch RK4 step with one dt per particle
+    (pusher.py:815-816), through track_batch and push_batch."""
+    wl = _dt_workload(tag)
+    np.testing.assert_array_equal(wl.r0, dt_golden[f"{tag}/r0"])
+    e, b = oracle_fields(wl)
+    dt = dt_golden[f"{tag}/dt"]
+    steps, rec = int(dt_golden[f"{tag}/nsteps"]), int(dt_golden[f"{tag}/rec"])
+    rh, vh, _ = orc.track_batch(alg, wl.species.q_over_m, wl.r0, wl.v0, e, b, steps, dt, rec)
+    assert rel_pos_err(rh, dt_golden[f"{tag}/{alg}/r_hist"], half_width(wl)) < TOL
+    assert rel_vel_err(vh, dt_golden[f"{tag}/{alg}/v_hist"]) < TOL
+    rn, vn = orc.push_step(alg, wl.r0, wl.v0, orc._Fields(e, b), 0.0, dt, wl.species.q_over_m)
+    np.testing.assert_allclose(rn, dt_golden[f"{tag}/{alg}/push_r"], rtol=1e-14)
+    np.testing.assert_allclose(vn, dt_golden[f"{tag}/{alg}/push_v"], rtol=1e-14)
+
+
+def test_particle_distribution_boundary_conversions(golden):
+    """The package's own ParticleDistribution (not the oracle's copy): the
+    reference's per-component v -> beta*gamma -> v conversions
+    (particles.py:71-117, :393-457) on the C1 final state."""
+    from pypatools_b200 import ParticleDistribution
+    x = golden["c1/boris/r_hist"][-1]
+    v = golden["c1/boris/v_hist"][-1]
+    pd = ParticleDistribution(species=IonSpecies("proton"), x_vec=x, p_vec=np.zeros_like(x), recalculate=False)
+    pd.set_p_from_v_vec(v)
+    np.testing.assert_allclose(pd.p_vec, golden["pd/p_vec"], rtol=1e-15, atol=0)
+    np.testing.assert_allclose(pd.v_vec, golden["pd/v_vec"], rtol=1e-15, atol=0)
+    np.testing.assert_array_equal(pd.x_vec, x)
