@@ -37,9 +37,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["rf_gap", "pusher_sweep", "sector_ring"], default="rf_gap",
+    ap.add_argument("--workload", choices=["rf_gap", "pusher_sweep", "sector_ring", "rf_gap_phases"],
+                    default="rf_gap",
                     help="rf_gap: the headline line (default); pusher_sweep: 1e6 electrons, Boris / vay_rel "
-                         "/ rk4_rel in both forms; sector_ring: 1e8 protons on a 512^3 Bz map")
+                         "/ rk4_rel / boris_rel / vay in both forms; sector_ring: 1e8 protons on a 512^3 Bz map; "
+                         "rf_gap_phases: the RF-gap job's map crossing and field-free drift on their own "
+                         "(--n particles, --nsteps steps per drift launch)")
     ap.add_argument("--n", type=int, default=None, help="particles (default: the workload's)")
     ap.add_argument("--nsteps", type=int, default=None, help="steps per job (default: the workload's)")
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -61,7 +64,7 @@ def parse():
                     help="skip the deposition, space-charge, electrode and loader objects")
     args = ap.parse_args()
     defaults = {"rf_gap": (10_000_000, 20_000), "pusher_sweep": (1_000_000, 10_000),
-                "sector_ring": (100_000_000, 50_000)}[args.workload]
+                "sector_ring": (100_000_000, 50_000), "rf_gap_phases": (1_000_000, 1000)}[args.workload]
     args.n = args.n or defaults[0]
     args.nsteps = args.nsteps or defaults[1]
     if args.sort_every is None:
@@ -144,6 +147,60 @@ def run_pusher_sweep(dev, n=1_000_000, nsteps=10_000, sort_every=100):
             "map": "129^3 over a 20 cm cube: E radial 1 MV/m at r = 0.1 m, Bz = 0.5 T cos(pi z / 0.2 m)",
             "error_metric": "per particle max over the start and end records of |r - r64| / max(|r64|, 0.1 m)",
             "sort_every": sort_every, "results": out}
+
+
+def run_phases(dev, n=1_000_000, nsteps=1000, sort_every=0, launches=4):
+    """The two phases of the RF-gap job, each on its own, for both forms:
+    the bunch as generated, every particle inside the map (100-step
+    launches after one cell sort, as the job's schedule runs the crossing),
+    and the same bunch moved 35 cm past the map, moving away (launches of
+    ``nsteps`` field-free steps, snapshots every 500 as in the job).  Device
+    time per launch (CUDA events); the last of ``launches`` launches is the
+    figure (the first ones warm up).  Snapshot rows are written as in the
+    job, so the drift figure is that of the job's 1000-step launches."""
+    import numpy as np
+    import torch
+    from pypatools_b200 import workloads, Field
+    from pypatools_b200.device_fields import DeviceFields
+    from pypatools_b200.pusher import DeviceTracker
+    phases = {"map": 100, "drift": nsteps}
+    wl = workloads.rf_gap_protons(n=n, nsteps=launches * max(phases.values()), rec_every=500)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    ef, bf = Field.from_arrays(g, wl.e_values), Field.from_arrays(g, wl.b_values)
+    out = {}
+    for form in ("mixed", "fp64"):
+        df = DeviceFields(ef, bf, form, dev)
+        for phase, k in phases.items():
+            r0 = wl.r0.copy()
+            if phase == "drift":
+                r0[:, 2] += 0.35
+            tr = DeviceTracker("boris", wl.species.q_over_m, df, n, launches * k, wl.dt, 500, form,
+                               rf_omega=2 * np.pi * wl.rf_frequency, rf_phase=torch.from_numpy(wl.rf_phase),
+                               device=dev)
+            tr.load(torch.from_numpy(r0).to(dev), torch.from_numpy(wl.v0).to(dev))
+            if phase == "map":
+                tr.sort()
+            ms = []
+            for _ in range(launches):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                tr.advance(k)
+                b.record()
+                torch.cuda.synchronize()
+                ms.append(a.elapsed_time(b))
+            out.setdefault(form, {})[phase] = {"steps_per_launch": k, "ms_per_launch": ms[-1],
+                                               "particle_steps_per_s": n * k / (ms[-1] / 1e3), "all_ms": ms}
+            del tr
+        del df
+        torch.cuda.empty_cache()
+    for phase in phases:
+        out[f"mixed_over_fp64_{phase}"] = (out["mixed"][phase]["particle_steps_per_s"] /
+                                           out["fp64"][phase]["particle_steps_per_s"])
+    return {"metric": "particle-steps/s per phase of the RF-gap job, mixed vs float64",
+            "workload": "rf_gap_protons", "particles": n, "launches": launches,
+            "phases": {"map": "the bunch as generated, inside the 256^3 map, cell-sorted once",
+                       "drift": "the bunch 35 cm past the map, moving away: every step field-free"},
+            "results": out}
 
 
 def run_sector_ring(dev, n=100_000_000, nsteps=50_000, sort_every=100):
@@ -406,14 +463,19 @@ def run_serving(n_jobs, device, rate=50.0):
         g = {"x": grid[0], "y": grid[1], "z": grid[2]}
         fields.append((Field.zero(3) if e is None else Field.from_arrays(g, e), Field.from_arrays(g, b)))
     specs = workloads.serving_stream(n_jobs=n_jobs, rate=rate)
-    warm = workloads.serving_stream(n_jobs=12, rate=rate, seed=40, n_max=1e4, steps_max=1500)
+    # one small job per (map, pusher) class: the stream's maps are resident
+    # before it starts, and every class kernel has run once
+    bunch = workloads.quad_solenoid_protons(n=256, nsteps=1, seed=40, nodes=2)
+    algs = ("boris", "vay_rel", "rk4_rel")
     out = {}
     for form in ("mixed", "fp64"):
         def jobs_of(sp):
             return [TrackingJob(s.job_id, ion.q_over_m, s.algorithm, s.r0, s.v0, *fields[s.map_index], s.nsteps,
                                 1e-11, precision=form, arrival=s.arrival) for s in sp]
-        TrackingServer(device=device, chunk=500).run(jobs_of(warm), realtime=False)   # kernels, graphs, maps
+        warm = [TrackingJob(i, ion.q_over_m, algs[i % 3], bunch.r0, bunch.v0, *fields[i // 3], 1200, 1e-11,
+                            precision=form, arrival=0.0) for i in range(3 * len(fields))]
         server = TrackingServer(device=device, budget_bytes=120e9, chunk=500)
+        server.run(warm, realtime=False)
         rep = server.run(jobs_of(specs), realtime=True)
         span = specs[-1].arrival
         rep["offered_particle_steps_per_s"] = sum(s.n * s.nsteps for s in specs) / span if span > 0 else None
@@ -568,7 +630,8 @@ def main():
     dev = torch.device("cuda", local)
     if args.workload != "rf_gap":
         if rank == 0:
-            fn = run_pusher_sweep if args.workload == "pusher_sweep" else run_sector_ring
+            fn = {"pusher_sweep": run_pusher_sweep, "sector_ring": run_sector_ring,
+                  "rf_gap_phases": run_phases}[args.workload]
             print(json.dumps(fn(dev, args.n, args.nsteps, args.sort_every)), flush=True)
         return
     if world > 1:

@@ -35,6 +35,7 @@
  *                   cylindrical-map loaders (field_loaders.py:612-640, :836-899)
  *   ppt_cell_sort   no reference counterpart: particle reordering for gather
  *                   locality (the reference has no particle ordering step)
+ *   ppt_restore_order  no reference counterpart: back to row order
  */
 #ifndef PPT_H
 #define PPT_H
@@ -333,6 +334,13 @@ int ppt_jobs_destroy(ppt_jobs* jobs);
 int64_t ppt_cell_sort_scratch_bytes(int64_t n);
 int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* order, double* rf_phase,
                   void* scratch, void* stream);
+
+/* Put particles back in row order (slot s moves to position order[s]) and
+ * set order to the identity: once a bunch has left its maps the cell order
+ * buys nothing, and in row order the snapshot rows are written coalesced.
+ * order must be a permutation of 0 .. n-1 (as ppt_cell_sort keeps it);
+ * scratch as for ppt_cell_sort.  Always permutes (the caller decides when). */
+int ppt_restore_order(ppt_state* st, int64_t* order, double* rf_phase, void* scratch, void* stream);
 
 /* Poisson mesh of the reference's space-charge solver: cells[d] nodes per
  * axis spaced extent[d] / cells[d], the first at -extent[d] / 2 (the

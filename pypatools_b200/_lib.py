@@ -105,6 +105,7 @@ SIGNATURES = {
     "ppt_track": (c_int, [POINTER(State), POINTER(Fields), POINTER(TrackArgs), c_void_p]),
     "ppt_cell_sort_scratch_bytes": (c_int64, [c_int64]),
     "ppt_cell_sort": (c_int, [POINTER(State), POINTER(Fields), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "ppt_restore_order": (c_int, [POINTER(State), c_void_p, c_void_p, c_void_p, c_void_p]),
     "ppt_moments_scratch_bytes": (c_int64, [c_int64]),
     "ppt_moments": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "ppt_moments_noalloc": (c_int, [c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p]),

@@ -19,6 +19,7 @@
 // reference counterpart: the reference runs one track_batch call at a time
 // (pusher.py:894-1012).
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "track_params.cuh"
@@ -60,6 +61,58 @@ static int layout_index(int layout) {
 }
 
 static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Class lanes (a non-blocking stream and its join event) and fork events
+// outlive the job tables that use them: a serving loop builds a table
+// whenever its job set changes (tens of times a second), and creating and
+// destroying a stream and an event per class each time cost more host time
+// than the tick itself.  Destroyed tables return theirs here, per device;
+// work still queued on a lane simply runs before the next table's.
+struct LanePool {
+    std::mutex mu;
+    std::vector<std::vector<cudaStream_t>> streams;   // by device ordinal
+    std::vector<std::vector<cudaEvent_t>> events;
+};
+
+static LanePool& lane_pool() {
+    static LanePool* p = new LanePool();   // never destroyed: its streams live as long as the process
+    return *p;
+}
+
+static cudaError_t take_stream(int dev, cudaStream_t* out) {
+    LanePool& P = lane_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        if ((int)P.streams.size() > dev && !P.streams[dev].empty()) {
+            *out = P.streams[dev].back();
+            P.streams[dev].pop_back();
+            return cudaSuccess;
+        }
+    }
+    return cudaStreamCreateWithFlags(out, cudaStreamNonBlocking);
+}
+
+static cudaError_t take_event(int dev, cudaEvent_t* out) {
+    LanePool& P = lane_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        if ((int)P.events.size() > dev && !P.events[dev].empty()) {
+            *out = P.events[dev].back();
+            P.events[dev].pop_back();
+            return cudaSuccess;
+        }
+    }
+    return cudaEventCreateWithFlags(out, cudaEventDisableTiming);
+}
+
+static void give_lanes(int dev, const std::vector<cudaStream_t>& streams, const std::vector<cudaEvent_t>& events) {
+    LanePool& P = lane_pool();
+    std::lock_guard<std::mutex> g(P.mu);
+    if ((int)P.streams.size() <= dev) P.streams.resize(dev + 1);
+    if ((int)P.events.size() <= dev) P.events.resize(dev + 1);
+    P.streams[dev].insert(P.streams[dev].end(), streams.begin(), streams.end());
+    P.events[dev].insert(P.events[dev].end(), events.begin(), events.end());
+}
 
 struct JobsLayout {
     size_t queues, steps, done, total, f64, mix, tindex, jindex, istart, bytes;
@@ -220,17 +273,18 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
         K.Q.chunk = 0;
         H->classes.push_back(K);
     }
-    // one stream per class beyond the first, which runs on the caller's stream
+    // one stream per class beyond the first, which runs on the caller's
+    // stream (lanes and events from the device's pool)
     H->fork = nullptr;
     if (H->classes.size() > 1) {
-        cudaError_t e = cudaEventCreateWithFlags(&H->fork, cudaEventDisableTiming);
+        cudaError_t e = take_event(H->device, &H->fork);
         for (size_t i = 1; e == cudaSuccess && i < H->classes.size(); ++i) {
             cudaStream_t st;
             cudaEvent_t ev;
-            e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+            e = take_stream(H->device, &st);
             if (e != cudaSuccess) break;
             H->lanes.push_back(st);
-            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            e = take_event(H->device, &ev);
             if (e != cudaSuccess) break;
             H->joins.push_back(ev);
         }
@@ -285,11 +339,11 @@ extern "C" int ppt_jobs_progress(const ppt_jobs* H, int64_t** steps, int32_t** d
 
 extern "C" int ppt_jobs_destroy(ppt_jobs* H) {
     if (!H) return PPT_OK;
-    // work still queued on the lanes completes first: destroying a stream or
-    // an event does not cancel it
-    for (cudaStream_t st : H->lanes) cudaStreamDestroy(st);
-    for (cudaEvent_t ev : H->joins) cudaEventDestroy(ev);
-    if (H->fork) cudaEventDestroy(H->fork);
+    // lanes and events go back to the device's pool; work still queued on a
+    // lane completes before anything a later table issues on it
+    std::vector<cudaEvent_t> events(H->joins);
+    if (H->fork) events.push_back(H->fork);
+    give_lanes(H->device, H->lanes, events);
     delete H;
     return PPT_OK;
 }

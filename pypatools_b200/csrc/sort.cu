@@ -204,6 +204,29 @@ __global__ void sort_copy_back(int64_t words, const uint32_t* __restrict__ src, 
         dst[i] = src[i];
 }
 
+// Back to row order: slot s goes to position order[s] (order is a
+// permutation of 0 .. n-1, kept so by the sorts), every state column and the
+// RF phase with it.  A value outside [0, n) is skipped rather than written.
+__global__ void restore_scatter(int64_t n, const int64_t* __restrict__ order, int ncols64,
+                                const double* __restrict__ src64, double* __restrict__ dst64, int na,
+                                const uint32_t* __restrict__ src_a, int nb, const uint32_t* __restrict__ src_b,
+                                uint32_t* __restrict__ dst32, const double* __restrict__ phase,
+                                double* __restrict__ phase_out) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int64_t d = order[s];
+    if (d < 0 || d >= n) return;
+    for (int c = 0; c < ncols64; ++c) dst64[c * n + d] = src64[c * n + s];
+    for (int c = 0; c < na; ++c) dst32[c * n + d] = src_a[c * n + s];
+    for (int c = 0; c < nb; ++c) dst32[(na + c) * n + d] = src_b[c * n + s];
+    if (phase) phase_out[d] = phase[s];
+}
+
+__global__ void iota_rows(int64_t n, int64_t* __restrict__ order) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s < n) order[s] = s;
+}
+
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SortLayout {
@@ -308,6 +331,36 @@ extern "C" int ppt_cell_sort(ppt_state* st, const ppt_fields* fields, int64_t* o
     }
     copy_back(order_tmp, order, (size_t)n * 8, ctrl, n, s);
     if (rf_phase) copy_back(phase_tmp, rf_phase, (size_t)n * 8, ctrl, n, s);
+    PPT_CUDA_TRY(cudaGetLastError());
+    return PPT_OK;
+}
+
+extern "C" int ppt_restore_order(ppt_state* st, int64_t* order, double* rf_phase, void* scratch, void* stream) {
+    int rc = check_state(st);
+    if (rc) return rc;
+    if (st->n == 0) return PPT_OK;
+    if (!order || !scratch) return fail(PPT_ERR_ARG, "order and scratch must not be NULL");
+    const int64_t n = st->n;
+    SortLayout L = sort_layout(n);
+    char* base = static_cast<char*>(scratch);
+    double* tmp64 = reinterpret_cast<double*>(base + L.tmp64);
+    uint32_t* tmp32 = reinterpret_cast<uint32_t*>(base + L.tmp32);
+    double* phase_tmp = reinterpret_cast<double*>(base + L.phase);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int block = 256;
+    if (st->precision == PPT_PREC_F64) {
+        restore_scatter<<<grid_for(n, block), block, 0, s>>>(n, order, 6, st->f64, tmp64, 0, nullptr, 0, nullptr,
+                                                             nullptr, rf_phase, phase_tmp);
+        PPT_CUDA_TRY(cudaMemcpyAsync(st->f64, tmp64, (size_t)n * 6 * 8, cudaMemcpyDeviceToDevice, s));
+    } else {
+        restore_scatter<<<grid_for(n, block), block, 0, s>>>(
+            n, order, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 12,
+            reinterpret_cast<const uint32_t*>(st->f32), tmp32, rf_phase, phase_tmp);
+        PPT_CUDA_TRY(cudaMemcpyAsync(st->i32, tmp32, (size_t)n * 3 * 4, cudaMemcpyDeviceToDevice, s));
+        PPT_CUDA_TRY(cudaMemcpyAsync(st->f32, tmp32 + 3 * n, (size_t)n * 12 * 4, cudaMemcpyDeviceToDevice, s));
+    }
+    if (rf_phase) PPT_CUDA_TRY(cudaMemcpyAsync(rf_phase, phase_tmp, (size_t)n * 8, cudaMemcpyDeviceToDevice, s));
+    iota_rows<<<grid_for(n, block), block, 0, s>>>(n, order);
     PPT_CUDA_TRY(cudaGetLastError());
     return PPT_OK;
 }

@@ -173,6 +173,7 @@ class DeviceTracker:
                 raise ValueError(f"dt must be a scalar or ({n},), got {tuple(d.shape)}")
             self.dt_rows = d.to(dev).contiguous().clone()
         self.order = None
+        self.row_order = False   # order is the identity (restore_order): the kernels need not read it
         self.sort_scratch = None
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.counters = torch.zeros(2, dtype=torch.int64, device=dev) if counters else None
@@ -182,12 +183,18 @@ class DeviceTracker:
         return _lib.stream_handle(stream)
 
     def load(self, r, v, stream=None):
-        """r, v: (n,3) float64 CUDA tensors."""
+        """r, v: (n,3) float64 CUDA tensors, loaded in row order."""
         dev = self.status.device
         check_rows(r, self.n, dev, "r")
         check_rows(v, self.n, dev, "v")
         _lib.check(self.lib.ppt_state_load(self.state, self.dfields.fields, r.data_ptr(), v.data_ptr(),
                                            self._stream(stream)))
+        if self.rf_phase is not None and self.order is not None and not self.row_order:
+            # the RF phases were permuted with the old state: back to rows
+            with self.torch.cuda.stream(stream if stream is not None else self.torch.cuda.current_stream()):
+                self.rf_phase.index_copy_(0, self.order, self.rf_phase.clone())
+        self.order = None           # slot s holds row s again
+        self.row_order = False
         self.launches += 1
 
     def advance(self, k, stream=None):
@@ -213,7 +220,7 @@ class DeviceTracker:
         a.rf_phase = self.rf_phase.data_ptr() if self.rf_phase is not None else None
         a.r_hist = self.r_hist.data_ptr() if self.r_hist is not None else None
         a.v_hist = self.v_hist.data_ptr() if self.v_hist is not None else None
-        a.order = self.order.data_ptr() if self.order is not None else None
+        a.order = self._order_ptr()
         a.status = self.status.data_ptr()
         a.counters = self.counters.data_ptr() if self.counters is not None else None
         if self.surface is not None:
@@ -240,6 +247,9 @@ class DeviceTracker:
         again.  The share comes from the device counters, copied to pinned
         memory after each launch and read with a lag: at most ``in_flight``
         launches are queued ahead, so the GPU never waits on the host.
+        Once a finished launch met no map at all, the particles go back to
+        row order (``restore_order``) for the snapshot rows' sake, until a
+        map holds particles again.
         ``after_launch(steps_done)`` runs after each launch is enqueued;
         ``launch_events`` (a list) receives (start event, end event, first
         step, steps) for each track launch."""
@@ -255,6 +265,7 @@ class DeviceTracker:
         last_hits = None
         dense = True            # the maps hold a good share of the particles
         sorted_sparse = False   # the grouping sort after the bunch left has been made
+        empty = False           # the newest finished launch met no map
         done = 0
         if nsteps == 0:
             self.advance(0, stream)
@@ -272,11 +283,14 @@ class DeviceTracker:
                             dense, sorted_sparse = True, False
                         else:
                             dense = False
+                        empty = hits == last_hits
                     last_hits = hits
                 if dense or not sorted_sparse:
                     if (self.step % sort_every == 0) or not dense:
                         self.sort(stream)
                     sorted_sparse = not dense
+                elif empty and not self.row_order:
+                    self.restore_order(stream)
                 k = min(sort_every if dense else long_chunk, chunk if dense else long_chunk, nsteps - done)
                 if dense:
                     k = min(k, sort_every - self.step % sort_every)
@@ -302,19 +316,39 @@ class DeviceTracker:
             if after_launch is not None:
                 after_launch(done)
 
-    def sort(self, stream=None):
-        """Reorder particles by cell (gather locality)."""
-        torch = self.torch
-        if not self.dfields.has_maps or self.n == 0:
-            return
+    def _order_ptr(self):
+        return None if self.order is None or self.row_order else self.order.data_ptr()
+
+    def _sort_scratch(self):
         if self.order is None:
-            self.order = torch.arange(self.n, dtype=torch.int64, device=self.device)
+            self.order = self.torch.arange(self.n, dtype=self.torch.int64, device=self.device)
         if self.sort_scratch is None:
             nbytes = self.lib.ppt_cell_sort_scratch_bytes(self.n)
-            self.sort_scratch = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self.sort_scratch = self.torch.empty(nbytes, dtype=self.torch.uint8, device=self.device)
+        return self.sort_scratch
+
+    def restore_order(self, stream=None):
+        """Put the particles back in row order (``ppt_restore_order``); the
+        order array becomes the identity and the kernels stop reading it."""
+        if self.n == 0 or self.order is None or self.row_order:
+            return
+        scratch = self._sort_scratch()
+        _lib.check(self.lib.ppt_restore_order(self.state, self.order.data_ptr(),
+                                              self.rf_phase.data_ptr() if self.rf_phase is not None else None,
+                                              scratch.data_ptr(), self._stream(stream)))
+        self.row_order = True
+        # scatter, one iota kernel (the copy-backs are memcpy calls)
+        self.launches += 2
+
+    def sort(self, stream=None):
+        """Reorder particles by cell (gather locality)."""
+        if not self.dfields.has_maps or self.n == 0:
+            return
+        scratch = self._sort_scratch()
+        self.row_order = False
         _lib.check(self.lib.ppt_cell_sort(self.state, self.dfields.fields, self.order.data_ptr(),
                                           self.rf_phase.data_ptr() if self.rf_phase is not None else None,
-                                          self.sort_scratch.data_ptr(), self._stream(stream)))
+                                          scratch.data_ptr(), self._stream(stream)))
         # keys, tile scan, top scan, scan add, scatter, then one copy-back per
         # permuted array (state block(s), order, RF phase)
         self.launches += 5 + (1 if self.precision == "fp64" else 2) + 1 + (1 if self.rf_phase is not None else 0)
@@ -324,8 +358,7 @@ class DeviceTracker:
         for t, name in ((r, "r"), (v, "v")):
             if t is not None:
                 check_rows(t, self.n, self.status.device, name)
-        _lib.check(self.lib.ppt_state_store(self.state, self.dfields.fields,
-                                            self.order.data_ptr() if self.order is not None else None,
+        _lib.check(self.lib.ppt_state_store(self.state, self.dfields.fields, self._order_ptr(),
                                             r.data_ptr() if r is not None else None,
                                             v.data_ptr() if v is not None else None, self._stream(stream)))
         self.launches += 1
@@ -340,21 +373,85 @@ class DeviceTracker:
         return {"map_hits": int(c[0]), "particle_steps": int(c[1])}
 
 
+class HostResultPool:
+    """Anonymous host mappings for results the GPU fills (``host_array``),
+    recycled once the caller drops the arrays built on them.
+
+    A fresh mapping costs its first touch: the kernel zeroes every page as
+    the results land (about 50 GB/s with 24 threads on a B200 host even with
+    transparent huge pages, against 145 GB/s for a copy into touched pages),
+    which for the 19.7 GB histories of a 1e7-particle track is slower than
+    the PCIe link.  When every array over a mapping has been released, the
+    mapping goes back to this pool, still touched, and the next request of
+    the same size takes it; the pool keeps at most ``limit`` bytes of free
+    mappings (``PPT_HOST_POOL_BYTES``, default 32 GiB; 0 disables it) and
+    unmaps the rest.  The results are always fully written before they are
+    returned, so a recycled mapping's earlier contents are never visible."""
+
+    def __init__(self, limit):
+        import threading
+        self.limit = int(limit)
+        self.free = {}          # nbytes -> [mmap, ...]
+        self.free_bytes = 0
+        self.lock = threading.RLock()   # a collection inside take() may call give()
+
+    def take(self, nbytes):
+        with self.lock:
+            maps = self.free.get(nbytes)
+            if maps:
+                self.free_bytes -= nbytes
+                return maps.pop()
+        m = mmap.mmap(-1, nbytes, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
+        try:
+            m.madvise(mmap.MADV_HUGEPAGE)
+        except (OSError, AttributeError):
+            pass        # transparent huge pages off: plain pages, still correct
+        return m
+
+    def give(self, m):
+        nbytes = len(m)
+        with self.lock:
+            if self.free_bytes + nbytes <= self.limit:
+                self.free.setdefault(nbytes, []).append(m)
+                self.free_bytes += nbytes
+        # over the limit: dropped here and unmapped with its last reference
+        # (the array's buffer export on it is released after this callback)
+
+    def clear(self):
+        """Drop every free mapping (unmapped as their references go)."""
+        with self.lock:
+            self.free, self.free_bytes = {}, 0
+
+
+def _pool_limit():
+    import os
+    try:
+        return int(float(os.environ.get("PPT_HOST_POOL_BYTES", 32 << 30)))
+    except ValueError:
+        return 32 << 30
+
+
+HOST_POOL = HostResultPool(_pool_limit())
+
+
 def host_array(shape, dtype=np.float64):
-    """A fresh numpy array for results the GPU fills, backed (from 64 MiB up)
-    by anonymous memory advised for transparent huge pages: writing tens of
-    GB into fresh 4 KiB pages is bound by page faults (27 GB/s measured with
-    24 threads on a B200 host), with huge pages the copies run at PCIe speed
-    (50 GB/s).  The array owns its mapping; it is released with the array."""
+    """A numpy array for results the GPU fills, backed (from 64 MiB up) by an
+    anonymous mapping advised for transparent huge pages, taken from
+    ``HOST_POOL``: writing tens of GB into fresh 4 KiB pages is bound by page
+    faults (27 GB/s measured with 24 threads on a B200 host), with huge pages
+    by their zeroing (50 GB/s), and into a recycled mapping by the copy
+    alone.  The mapping returns to the pool when the array and every view of
+    it are gone."""
+    import weakref
     nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
     if nbytes < (64 << 20) or not hasattr(mmap, "MADV_HUGEPAGE"):
         return np.empty(shape, dtype)
-    m = mmap.mmap(-1, nbytes, flags=mmap.MAP_PRIVATE | mmap.MAP_ANONYMOUS)
-    try:
-        m.madvise(mmap.MADV_HUGEPAGE)
-    except OSError:
-        pass            # transparent huge pages off: plain pages, still correct
-    return np.frombuffer(m, dtype=dtype).reshape(shape)
+    m = HOST_POOL.take(nbytes)
+    base = np.frombuffer(m, dtype=dtype)
+    # views of the result keep `base` alive; once it is collected its buffer
+    # export on m is released and m can serve the next request
+    weakref.finalize(base, HOST_POOL.give, m)
+    return base.reshape(shape)
 
 
 class HostStager:

@@ -96,6 +96,7 @@ class TrackingServer:
         self._handle = None
         self._scratch = None
         self._graph = None
+        self._h_cap = 0
         self.ticks = 0
         self.rebuilds = 0
         self.graph_captures = 0
@@ -116,8 +117,11 @@ class TrackingServer:
             tr = DeviceTracker(job.algorithm, job.q_over_m, df, job.n, job.nsteps, job.dt, job.rec_every,
                                job.precision, rf_omega=rf_omega, rf_phase=rf_phase, t0=job.t0, record=True,
                                device=self.device)
-            r = torch.from_numpy(job.r0).to(self.device)
-            v = torch.from_numpy(job.v0).to(self.device)
+            # through pinned host blocks (torch's caching host allocator keeps
+            # each block until its copy is done): a copy from pageable memory
+            # holds the host thread for the whole transfer
+            r = torch.from_numpy(job.r0).pin_memory().to(self.device, non_blocking=True)
+            v = torch.from_numpy(job.v0).pin_memory().to(self.device, non_blocking=True)
             tr.load(r, v, stream=self.upload)
         job._tracker, job._fields = tr, df
         job.t_admit = now
@@ -169,8 +173,14 @@ class TrackingServer:
         so, do = steps.value - base, done.value - base
         self._d_steps = self._scratch[so:so + 8 * n].view(torch.int64)
         self._d_done = self._scratch[do:do + 4 * n].view(torch.int32)
-        self._h_steps = torch.empty(n, dtype=torch.int64, pin_memory=True)
-        self._h_done = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        if self._h_cap < n:
+            # pinned progress buffers, grown (never per table: a pinned
+            # allocation costs more host time than a tick)
+            self._h_cap = max(n, 2 * self._h_cap)
+            self._h_steps_buf = torch.empty(self._h_cap, dtype=torch.int64, pin_memory=True)
+            self._h_done_buf = torch.empty(self._h_cap, dtype=torch.int32, pin_memory=True)
+        self._h_steps = self._h_steps_buf[:n]
+        self._h_done = self._h_done_buf[:n]
         self.rebuilds += 1
 
     def _capture(self):
@@ -239,6 +249,7 @@ class TrackingServer:
         sleeping.  Returns a report dict; each job gets t_admit, t_done,
         r_hist, v_hist."""
         torch = self.torch
+        base = (self.ticks, self.rebuilds, self.graph_captures, self.graph_replays)
         for j in jobs:
             j.reset()
         pending = collections.deque(sorted(jobs, key=lambda j: j.arrival))
@@ -321,7 +332,8 @@ class TrackingServer:
                 "p50_latency_s": float(np.percentile(lat, 50)) if lat.size else None,
                 "p99_latency_s": float(np.percentile(lat, 99)) if lat.size else None,
                 "max_latency_s": float(lat.max()) if lat.size else None,
-                "ticks": self.ticks, "rebuilds": self.rebuilds, "graph_captures": self.graph_captures,
-                "graph_replays": self.graph_replays, "gpu_tick_s": gpu_tick_ms / 1e3,
+                "ticks": self.ticks - base[0], "rebuilds": self.rebuilds - base[1],
+                "graph_captures": self.graph_captures - base[2], "graph_replays": self.graph_replays - base[3],
+                "gpu_tick_s": gpu_tick_ms / 1e3,
                 "gpu_busy_fraction": gpu_tick_ms / 1e3 / wall if wall > 0 else 0.0,
                 "host_s": {k: round(v, 4) for k, v in host.items()}}

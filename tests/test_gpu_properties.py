@@ -120,3 +120,42 @@ def test_nonfinite_input_warns(cuda):
     with pytest.warns(RuntimeWarning, match="non-finite"):
         rh, _, _ = PusherGPU(wl.species, "boris").track_batch(r0, wl.v0, e, b, 5, wl.dt)
     assert np.isnan(rh[-1, 1, 0]) and np.isfinite(rh[-1, 0]).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_row_order_restored_after_the_bunch_leaves(cuda, precision):
+    """The launch schedule sorts the RF-gap bunch by cell while it crosses the
+    map, then puts it back in row order (ppt_restore_order) once a launch met
+    no map: the histories, the final state and the RF phases are those of the
+    unsorted run, bit for bit."""
+    import torch
+    from pypatools_b200.device_fields import DeviceFields
+    from pypatools_b200.pusher import DeviceTracker
+    n, nsteps = 4096, 2500
+    wl = workloads.rf_gap_protons(n=n, nsteps=nsteps, nodes=64, rec_every=100)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    df = DeviceFields(Field.from_arrays(g, wl.e_values), Field.from_arrays(g, wl.b_values), precision, cuda)
+    r0 = torch.from_numpy(wl.r0).to(cuda)
+    v0 = torch.from_numpy(wl.v0).to(cuda)
+    out = {}
+    for sort_every in (0, 100):
+        tr = DeviceTracker("boris", wl.species.q_over_m, df, n, nsteps, wl.dt, wl.rec_every, precision,
+                           rf_omega=2 * np.pi * wl.rf_frequency, rf_phase=torch.from_numpy(wl.rf_phase),
+                           counters=True, device=cuda)
+        tr.load(r0, v0)
+        tr.run(nsteps, 100, sort_every=sort_every, long_chunk=200)
+        r = torch.empty_like(r0)
+        v = torch.empty_like(v0)
+        tr.store(r, v)
+        torch.cuda.synchronize()
+        out[sort_every] = (tr.r_hist.cpu(), tr.v_hist.cpu(), r.cpu(), v.cpu(), tr.rf_phase.cpu(), tr)
+    base, srt = out[0], out[100]
+    tr = srt[5]
+    assert tr.row_order and torch.equal(tr.order.cpu(), torch.arange(n))
+    for a, b in zip(base[:5], srt[:5]):
+        assert torch.equal(a, b)
+    assert bool(torch.all(base[0][-1, :, 2] > wl.grid[2][-1]))     # every proton left through the far face
+    # a second job on the same tracker starts from row order again
+    tr.step = 0
+    tr.load(r0, v0)
+    assert tr.order is None and not tr.row_order

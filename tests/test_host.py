@@ -244,3 +244,42 @@ def test_tracking_job_arguments_checked_at_submission():
         TrackingJob(0, 1.0, "boris", np.zeros(15), np.zeros(15), None, None, 100, 1e-11)
     with pytest.raises(ValueError, match="rec_every"):
         TrackingJob(0, 1.0, "boris", r, r, None, None, 100, 1e-11, rec_every=0)
+
+
+def test_host_result_pool_recycles_released_mappings():
+    """track_batch's numpy results sit on pooled mappings: one goes back to
+    the pool only when the array and every view of it are gone, is handed out
+    again for the same size, and the pool keeps no more than its limit."""
+    import gc
+    from pypatools_b200.pusher import HostResultPool, host_array
+    import pypatools_b200.pusher as pusher_mod
+    saved = pusher_mod.HOST_POOL
+    size = 3 * (1 << 22) * 3 * 8                        # 288 MiB
+    pool = pusher_mod.HOST_POOL = HostResultPool(2 * size)
+    try:
+        shape = (3, 1 << 22, 3)
+        a = host_array(shape)
+        assert a.shape == shape and a.dtype == np.float64 and a.flags.writeable
+        addr = a.ctypes.data
+        a[:] = 1.0
+        view = a[1]
+        del a
+        gc.collect()
+        assert pool.free_bytes == 0                     # the view still holds it
+        del view
+        gc.collect()
+        assert pool.free_bytes == size
+        b = host_array(shape)
+        assert b.ctypes.data == addr and pool.free_bytes == 0
+        c = host_array(shape)
+        assert c.ctypes.data != addr
+        d = host_array(shape)
+        del b, c, d
+        gc.collect()
+        assert pool.free_bytes == 2 * size              # the third was over the limit: unmapped
+        small = host_array((10, 3))                     # below 64 MiB: plain numpy
+        assert small.base is None
+        pool.clear()
+        assert pool.free_bytes == 0
+    finally:
+        pusher_mod.HOST_POOL = saved
