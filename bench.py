@@ -73,13 +73,16 @@ def parse():
 
 
 # DRAM bytes per particle per launch of the mixed track kernel, from the ncu
-# capture of a 100-step in-map launch on the RF-gap workload at 1e6 protons
-# (the state read and written; the map's occupied cells stay in L1/L2).
-MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = 65.2
+# captures of `bench.py --workload rf_gap_phases` at 1e6 protons: a 100-step
+# launch inside the map (the 60 B state read and written; the map's occupied
+# cells stay in L1/L2) and a 1000-step field-free launch (the state and two
+# 48 B snapshot rows).
+MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = {"map": 126.9, "drift": 166.7}
 # Warp-instructions issued per warp-step (32 particle-steps) by the mixed
 # Boris kernel on the RF-gap layout, in the map and in field-free drift
-# (ncu smsp__inst_executed of one launch / warps / steps).
-WARP_INST_PER_WARP_STEP = {"map": 205.0, "drift": 13.0}
+# (ncu smsp__inst_executed of those launches / warps / steps).
+WARP_INST_PER_WARP_STEP = {"map": 249.7, "drift": 4.5}
+MIXED_STATE_BYTES = 60
 
 
 def _timed_track(tr, r0, v0, nsteps, sort_every, phase=None):
@@ -757,11 +760,14 @@ def main():
     psteps = m["counters"]["particle_steps"]
     n_launch = len(m["launch_ms"])
     gather_b = hits * 8 * m["n_comp"] * 4
-    state_b = n_launch * n * 2 * 48
+    state_b = n_launch * n * 2 * MIXED_STATE_BYTES
     snap_b = args.steps * (wl.nsteps // wl.rec_every + 1) * n * 48
     alg_bytes_per_launch = (gather_b + state_b + snap_b) / max(n_launch, 1)
     kernel_s = float(np.sum(m["launch_ms"])) / 1e3
     avg_launch_s = kernel_s / max(n_launch, 1)
+    n_map_launch = sum(1 for s0 in m["launch_step0"] if s0 < in_map_steps)
+    traffic_per_launch = n * (n_map_launch * MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH["map"] +
+                              (n_launch - n_map_launch) * MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH["drift"]) / max(n_launch, 1)
     achieved = alg_bytes_per_launch / avg_launch_s / 1e9
     clk_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
     n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
@@ -775,10 +781,11 @@ def main():
                 "basis": "algorithmic bytes (in-map corner gathers of the stored components + state + snapshot "
                          "rows) at the measured HBM copy bandwidth; the gathers are L1-served, so this is not "
                          "the kernel's limit (see limiter)",
-                "traffic": MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH * n,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one in-map 100-step launch "
-                                  "at 1e6 protons (profiles/track_mixed_kernel_rf_gap_1e6_in_map.txt), scaled "
-                                  "by particle count",
+                "traffic": traffic_per_launch,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 100-step in-map and a "
+                                  "1000-step field-free launch at 1e6 protons "
+                                  "(profiles/track_mixed_kernel_rf_gap_1e6_in_map.txt, *_drift.txt), scaled by "
+                                  "particle count and averaged over this job's launches of each kind",
                 "peak_kind": f"{peak_kind} hbm_gbs",
                 "kernel": "track_mixed_kernel<BORIS,RF,Ez|Bz layout>", "avg_launch_ms": avg_launch_s * 1e3,
                 "in_map_fraction": hits / max(1, psteps),

@@ -131,17 +131,18 @@ def test_row_order_restored_after_the_bunch_leaves(cuda, precision):
     import torch
     from pypatools_b200.device_fields import DeviceFields
     from pypatools_b200.pusher import DeviceTracker
+    dev = torch.device("cuda", 0)
     n, nsteps = 4096, 2500
     wl = workloads.rf_gap_protons(n=n, nsteps=nsteps, nodes=64, rec_every=100)
     g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
-    df = DeviceFields(Field.from_arrays(g, wl.e_values), Field.from_arrays(g, wl.b_values), precision, cuda)
-    r0 = torch.from_numpy(wl.r0).to(cuda)
-    v0 = torch.from_numpy(wl.v0).to(cuda)
+    df = DeviceFields(Field.from_arrays(g, wl.e_values), Field.from_arrays(g, wl.b_values), precision, dev)
+    r0 = torch.from_numpy(wl.r0).to(dev)
+    v0 = torch.from_numpy(wl.v0).to(dev)
     out = {}
     for sort_every in (0, 100):
         tr = DeviceTracker("boris", wl.species.q_over_m, df, n, nsteps, wl.dt, wl.rec_every, precision,
                            rf_omega=2 * np.pi * wl.rf_frequency, rf_phase=torch.from_numpy(wl.rf_phase),
-                           counters=True, device=cuda)
+                           counters=True, device=dev)
         tr.load(r0, v0)
         tr.run(nsteps, 100, sort_every=sort_every, long_chunk=200)
         r = torch.empty_like(r0)

@@ -44,7 +44,7 @@ def _check_alone(ion, jobs):
 def test_serving_results_same_alone_and_in_mix(cuda):
     fields = _map_fields()
     ion, jobs = _jobs(fields)
-    server = TrackingServer(chunk=32, use_graphs=True)
+    server = TrackingServer(chunk=32, use_graphs=True, capture_after=1)
     rep = server.run(jobs, realtime=False)
     assert rep["jobs"] == len(jobs)
     assert rep["graph_replays"] > 0 and rep["rebuilds"] >= 2
@@ -72,7 +72,7 @@ def test_serving_realtime_stream_with_graphs(cuda):
     # up to 1500 steps: the bunches leave their maps, so field-free runs are
     # split by the 16-step ticks here and by whole-track launches alone
     ion, jobs = _jobs(fields, n_jobs=24, spacing=0.004, steps_max=1500)
-    server = TrackingServer(chunk=16, use_graphs=True)
+    server = TrackingServer(chunk=16, use_graphs=True, capture_after=1)
     rep = server.run(jobs, realtime=True)
     assert rep["jobs"] == len(jobs)
     assert server.used_bytes == 0
