@@ -466,6 +466,7 @@ def run_serving(n_jobs, device, rate=50.0):
         g = {"x": grid[0], "y": grid[1], "z": grid[2]}
         fields.append((Field.zero(3) if e is None else Field.from_arrays(g, e), Field.from_arrays(g, b)))
     specs = workloads.serving_stream(n_jobs=n_jobs, rate=rate)
+    warm_stream = workloads.serving_stream(n_jobs=min(n_jobs, 100), rate=rate, seed=41)
     # one small job per (map, pusher) class: the stream's maps are resident
     # before it starts, and every class kernel has run once
     bunch = workloads.quad_solenoid_protons(n=256, nsteps=1, seed=40, nodes=2)
@@ -479,6 +480,10 @@ def run_serving(n_jobs, device, rate=50.0):
                             precision=form, arrival=0.0) for i in range(3 * len(fields))]
         server = TrackingServer(device=device, budget_bytes=120e9, chunk=500)
         server.run(warm, realtime=False)
+        # and a short stream of another seed, so the allocators' pools (device
+        # and pinned host blocks) hold the stream's sizes, as in a server that
+        # has been running
+        server.run(jobs_of(warm_stream), realtime=False)
         rep = server.run(jobs_of(specs), realtime=True)
         span = specs[-1].arrival
         rep["offered_particle_steps_per_s"] = sum(s.n * s.nsteps for s in specs) / span if span > 0 else None

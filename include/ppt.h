@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define PPT_ABI_VERSION 3
+#define PPT_ABI_VERSION 4
 
 /* status codes */
 #define PPT_OK               0
@@ -302,6 +302,7 @@ typedef struct {
     double* v_hist;
     int32_t* status;          /* device int32 or NULL */
     int64_t steps_done;       /* steps already taken (a table rebuilt mid-track resumes here) */
+    int64_t tick_steps;       /* steps this job advances per tick; 0 = the tick's chunk */
 } ppt_job_desc;
 
 typedef struct ppt_jobs ppt_jobs;   /* opaque host handle */
@@ -314,8 +315,8 @@ int64_t ppt_jobs_scratch_bytes(int n_jobs);
  * descriptors' device buffers must outlive the handle too. */
 int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scratch, ppt_jobs** out, void* stream);
 
-/* Advance every unfinished job by up to chunk steps (Boris-family half steps
- * and snapshots exactly as ppt_track).  Reads no host data and does not
+/* Advance every unfinished job by up to chunk steps (its tick_steps when
+ * that is set; Boris-family half steps and snapshots exactly as ppt_track).  Reads no host data and does not
  * synchronise: a captured CUDA graph of this call can be replayed. */
 int ppt_jobs_tick(ppt_jobs* jobs, int64_t chunk, void* stream);
 

@@ -16,7 +16,7 @@ ERRORS = {-1: "PPT_ERR_ARG", -2: "PPT_ERR_OOM", -3: "PPT_ERR_CUDA", -4: "PPT_ERR
 
 ALG_IDS = {"leapfrog": 0, "boris": 1, "rk4": 2, "yoshida": 3, "vay_rel": 4, "rk4_rel": 5,
            "yoshida_rel": 6, "boris_rel": 7, "vay": 8}
-ABI_VERSION = 3
+ABI_VERSION = 4
 PREC_F64, PREC_MIXED = 0, 1
 DTYPE_F64, DTYPE_F32 = 0, 1
 TRACK_INIT, TRACK_FINAL = 1, 2
@@ -65,7 +65,7 @@ class JobDesc(ctypes.Structure):
     _fields_ = [("state", State), ("fields", Fields), ("nsteps_total", c_int64), ("rec_every", c_int64),
                 ("dt", c_double), ("q_over_m", c_double), ("t0", c_double), ("rf_omega", c_double),
                 ("rf_phase", c_void_p), ("r_hist", c_void_p), ("v_hist", c_void_p), ("status", c_void_p),
-                ("steps_done", c_int64)]
+                ("steps_done", c_int64), ("tick_steps", c_int64)]
 
 
 # name -> (restype, argtypes); every symbol include/ppt.h declares

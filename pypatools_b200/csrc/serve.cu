@@ -44,6 +44,7 @@ struct ppt_jobs {
     int64_t* d_steps;
     int* d_done;
     const int64_t* d_total;
+    const int64_t* d_window;
 };
 
 namespace ppt {
@@ -115,7 +116,7 @@ static void give_lanes(int dev, const std::vector<cudaStream_t>& streams, const 
 }
 
 struct JobsLayout {
-    size_t queues, steps, done, total, f64, mix, tindex, jindex, istart, bytes;
+    size_t queues, steps, done, total, window, f64, mix, tindex, jindex, istart, bytes;
 };
 
 static JobsLayout jobs_layout(int n) {
@@ -125,6 +126,7 @@ static JobsLayout jobs_layout(int n) {
     L.steps = o;  o += al(sizeof(int64_t) * n);
     L.done = o;   o += al(sizeof(int) * n);
     L.total = o;  o += al(sizeof(int64_t) * n);
+    L.window = o; o += al(sizeof(int64_t) * n);
     L.f64 = o;    o += al(sizeof(TrackDev) * n);
     L.mix = o;    o += al(sizeof(TrackMixDev) * n);
     L.tindex = o; o += al(sizeof(int) * n);
@@ -135,11 +137,13 @@ static JobsLayout jobs_layout(int n) {
 }
 
 __global__ void jobs_advance_kernel(int n, int64_t* __restrict__ steps, int* __restrict__ done,
-                                    const int64_t* __restrict__ total, int64_t chunk) {
+                                    const int64_t* __restrict__ total, const int64_t* __restrict__ window,
+                                    int64_t chunk) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n || done[j]) return;
+    const int64_t w = window[j] > 0 ? window[j] : chunk;
     int64_t k = total[j] - steps[j];
-    if (k > chunk) k = chunk;
+    if (k > w) k = w;
     steps[j] += k;
     if (steps[j] >= total[j]) done[j] = 1;
 }
@@ -217,6 +221,7 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
     TrackDev* f64 = reinterpret_cast<TrackDev*>(img + L.f64);
     TrackMixDev* mix = reinterpret_cast<TrackMixDev*>(img + L.mix);
     int64_t* total = reinterpret_cast<int64_t*>(img + L.total);
+    int64_t* window = reinterpret_cast<int64_t*>(img + L.window);
     int* tindex = reinterpret_cast<int*>(img + L.tindex);
     int* jindex = reinterpret_cast<int*>(img + L.jindex);
     int* istart = reinterpret_cast<int*>(img + L.istart);
@@ -233,6 +238,11 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
             delete H;
             return fail(PPT_ERR_ARG, "steps_done must be in [0, nsteps_total]");
         }
+        if (jobs[j].tick_steps < 0 || jobs[j].tick_steps > 0x7fffffff) {
+            delete H;
+            return fail(PPT_ERR_ARG, "tick_steps must be in [0, 2^31)");
+        }
+        window[j] = jobs[j].tick_steps;
         reinterpret_cast<int64_t*>(img + L.steps)[j] = jobs[j].steps_done;
         const int rf = jobs[j].rf_phase != nullptr;
         const int lay = layout_index(jobs[j].state.precision == PPT_PREC_MIXED ? mix[j].map.layout
@@ -270,6 +280,7 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
         K.Q.queue = reinterpret_cast<unsigned*>(dev + L.queues) + (int)H->classes.size();
         K.Q.steps = reinterpret_cast<const int64_t*>(dev + L.steps);
         K.Q.done = reinterpret_cast<const int*>(dev + L.done);
+        K.Q.window = reinterpret_cast<const int64_t*>(dev + L.window);
         K.Q.chunk = 0;
         H->classes.push_back(K);
     }
@@ -297,6 +308,7 @@ extern "C" int ppt_jobs_create(const ppt_job_desc* jobs, int n_jobs, void* scrat
     H->d_steps = reinterpret_cast<int64_t*>(dev + L.steps);
     H->d_done = reinterpret_cast<int*>(dev + L.done);
     H->d_total = reinterpret_cast<const int64_t*>(dev + L.total);
+    H->d_window = reinterpret_cast<const int64_t*>(dev + L.window);
     cudaError_t e = cudaMemcpyAsync(scratch, img, L.bytes, cudaMemcpyHostToDevice, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) {
         ppt_jobs_destroy(H);
@@ -325,7 +337,8 @@ extern "C" int ppt_jobs_tick(ppt_jobs* H, int64_t chunk, void* stream) {
         if (i > 0) PPT_CUDA_TRY(cudaEventRecord(H->joins[i - 1], cs));
     }
     for (size_t i = 1; i < H->classes.size(); ++i) PPT_CUDA_TRY(cudaStreamWaitEvent(s, H->joins[i - 1], 0));
-    jobs_advance_kernel<<<(H->n_jobs + 255) / 256, 256, 0, s>>>(H->n_jobs, H->d_steps, H->d_done, H->d_total, chunk);
+    jobs_advance_kernel<<<(H->n_jobs + 255) / 256, 256, 0, s>>>(H->n_jobs, H->d_steps, H->d_done, H->d_total,
+                                                                H->d_window, chunk);
     PPT_CUDA_TRY(cudaGetLastError());
     return PPT_OK;
 }

@@ -572,10 +572,19 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
     return (unsigned)P.nsteps;
 }
 
+// Blocks of 128 per SM the launch bounds ask for: the Boris family's kernels
+// of a pruned record layout fit 80 registers without spills (6 blocks: the
+// RF-gap map crossing 65.0 -> 62.9 ms against 96 registers and 5 blocks);
+// the run-time dispatch, the full record and the collision test would spill
+// there and keep 5.
+__host__ __device__ constexpr int f64_min_blocks(int alg, bool coll, int layout) {
+    return !alg_skips_free(alg) ? 1 : (!coll && layout != 0 && layout != kLayFull) ? 6 : 5;
+}
+
 // L = 0: any fields; L = a kLay* mask: one uniform-grid map of that record
 // layout, no constant parts (fields_at, boris_v_m).
 template <int ALG, bool RF, bool COLL, int L>
-__global__ void __launch_bounds__(128, alg_skips_free(ALG) ? 5 : 1) track_f64_kernel(const __grid_constant__ TrackDev P) {
+__global__ void __launch_bounds__(128, f64_min_blocks(ALG, COLL, L)) track_f64_kernel(const __grid_constant__ TrackDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
     Ctx c = make_ctx(P);

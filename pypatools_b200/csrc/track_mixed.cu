@@ -1319,10 +1319,12 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
             MixCtx c{&sP, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
             if constexpr (RF) {
-                // this job's step window, when the launch reserved a table for it
+                // this job's step window, when the launch reserved a table
+                // that long for it (chunk + 1 entries; a job with a longer
+                // window of its own computes the same values directly)
                 extern __shared__ float4 rf_tab[];
                 const int nt = (int)sP.nsteps + 1;
-                if (Q.chunk + 1 <= kRfTable && nt <= kRfTable) {
+                if (Q.chunk + 1 <= kRfTable && nt <= Q.chunk + 1) {
                     build_rf_table(rf_tab, sP.step0, nt, sP.wdt);
                     c.tab = rf_tab;
                     c.tab0 = sP.step0;

@@ -92,6 +92,7 @@ struct JobQueueDev {
     unsigned* queue;          // work-queue head, zeroed before each tick
     const int64_t* steps;     // steps done per global job
     const int* done;          // 1 once the job's last step ran
+    const int64_t* window;    // steps per tick per global job (0: chunk)
     int64_t chunk;            // steps per tick
 };
 
@@ -167,8 +168,9 @@ __device__ __forceinline__ void block_add_counters(unsigned long long* counters,
 __device__ __forceinline__ void job_window(const JobQueueDev& Q, int gjob, int64_t total, int64_t* step0,
                                            int64_t* k, int* flags) {
     const int64_t s0 = Q.steps[gjob];
+    const int64_t w = Q.window[gjob] > 0 ? Q.window[gjob] : Q.chunk;
     int64_t kk = total - s0;
-    if (kk > Q.chunk) kk = Q.chunk;
+    if (kk > w) kk = w;
     if (kk < 0) kk = 0;
     *step0 = s0;
     *k = kk;

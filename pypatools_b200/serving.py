@@ -12,8 +12,9 @@ field map, a step count) arrive over time.  The loop
   ``ppt_jobs_tick`` -- one persistent kernel per (form, algorithm, RF, map
   layout) class, the classes on concurrent streams, whose blocks take (job,
   128-particle block) items from a device work queue, then a step-counter
-  kernel.  Once a job set has run ``capture_after`` ticks unchanged, its tick
-  is captured in a CUDA graph and replayed until the set changes;
+  kernel.  With ``use_graphs``, once a job set has run ``capture_after`` ticks
+  unchanged, its tick is captured in a CUDA graph and replayed until the set
+  changes;
 * retires jobs whose done flag is set: their histories are copied to the host
   while the next tick runs; a job's latency ends when its results are on the
   host.
@@ -80,14 +81,24 @@ class TrackingJob:
 
 
 class TrackingServer:
-    def __init__(self, device=None, budget_bytes=120e9, chunk=500, use_graphs=True, capture_after=16):
-        """``capture_after``: unchanged ticks before a job set's tick is
-        captured as a CUDA graph.  A capture drains the stream and costs about
-        0.7 ms of host time, a replay saves about as much as issuing the tick's
-        ~20 launches directly (0.05 ms): on the 2000-job serving stream, whose
+    def __init__(self, device=None, budget_bytes=120e9, chunk=500, use_graphs=False, capture_after=16,
+                 small_bunch=65536, max_boost=8):
+        """``use_graphs``, ``capture_after``: capture a job set's tick as a
+        CUDA graph once the set has run ``capture_after`` ticks unchanged.  Off
+        by default: issuing a tick's ~20 launches directly costs 0.05 ms of
+        host time, so a replay saves little, while a capture stalls the loop
+        (0.7 ms per capture after one unchanged tick, 20-33 ms per capture of
+        the larger job sets after 16): on the 2000-job serving stream, whose
         job set changes every 4 ticks on average, capturing after one unchanged
-        tick raised p99 latency from 0.41 to 0.64 s.  Graphs pay off for long
-        runs of an unchanged set."""
+        tick raised p99 latency from 0.41 to 0.64 s.
+
+        ``small_bunch``, ``max_boost``: a job of n < small_bunch particles
+        advances chunk * small_bunch / n steps per tick (at most max_boost
+        chunks), the rest ``chunk``.  A tick lasts as long as its largest
+        jobs' work, so with equal step windows a small bunch with many steps
+        waits through as many long ticks as a large one; its blocks are few,
+        so a longer window costs the tick little.  A job's results do not
+        depend on its windows (tracks are split-invariant bit for bit)."""
         torch = _torch()
         self.torch = torch
         self.lib = _lib.load()
@@ -96,6 +107,8 @@ class TrackingServer:
         self.chunk = int(chunk)
         self.use_graphs = use_graphs
         self.capture_after = max(1, int(capture_after))
+        self.small_bunch = int(small_bunch)
+        self.max_boost = max(1, int(max_boost))
         self.fields = FieldCache(capacity=16)
         self.compute = torch.cuda.Stream(device=self.device)
         self.upload = torch.cuda.Stream(device=self.device)
@@ -152,7 +165,14 @@ class TrackingServer:
         d.v_hist = tr.v_hist.data_ptr()
         d.status = tr.status.data_ptr()
         d.steps_done = job.steps_done
+        d.tick_steps = self._tick_steps(job)
         return d
+
+    def _tick_steps(self, job):
+        if job.n >= self.small_bunch:
+            return 0
+        boost = min(float(self.max_boost), self.small_bunch / max(job.n, 1))
+        return int(self.chunk * boost)
 
     # -- job table and graph -----------------------------------------------------
     def _rebuild(self):

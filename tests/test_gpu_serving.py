@@ -44,7 +44,9 @@ def _check_alone(ion, jobs):
 def test_serving_results_same_alone_and_in_mix(cuda):
     fields = _map_fields()
     ion, jobs = _jobs(fields)
-    server = TrackingServer(chunk=32, use_graphs=True, capture_after=1)
+    # equal step windows (no small-bunch boost): every job runs several ticks,
+    # so unchanged job sets are captured and replayed
+    server = TrackingServer(chunk=32, use_graphs=True, capture_after=1, small_bunch=0)
     rep = server.run(jobs, realtime=False)
     assert rep["jobs"] == len(jobs)
     assert rep["graph_replays"] > 0 and rep["rebuilds"] >= 2
@@ -78,3 +80,20 @@ def test_serving_realtime_stream_with_graphs(cuda):
     assert server.used_bytes == 0
     assert rep["p99_latency_s"] is not None and rep["p99_latency_s"] >= rep["p50_latency_s"] > 0
     _check_alone(ion, jobs)
+
+
+def test_serving_per_job_windows(cuda):
+    """Small bunches take longer step windows per tick (tick_steps): they
+    finish in fewer ticks than the others and their results are still those
+    of the job run alone, bit for bit."""
+    fields = _map_fields()
+    ion, jobs = _jobs(fields, n_jobs=8, spacing=0.0)
+    server = TrackingServer(chunk=32, use_graphs=False, small_bunch=1 << 20, max_boost=8)
+    windows = {j.job_id: server._tick_steps(j) for j in jobs}
+    assert all(w > 32 for w in windows.values())
+    rep = server.run(jobs, realtime=False)
+    assert rep["jobs"] == len(jobs)
+    longest = max(j.nsteps for j in jobs)
+    assert rep["ticks"] < -(-longest // 32)          # fewer ticks than equal 32-step windows need
+    _check_alone(ion, jobs)
+

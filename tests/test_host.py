@@ -28,7 +28,7 @@ def test_library_exports_every_header_symbol():
     for s in syms:
         assert hasattr(lib, s), s
     assert set(syms) == set(_lib.SIGNATURES)
-    assert lib.ppt_abi_version() == _lib.ABI_VERSION == 3
+    assert lib.ppt_abi_version() == _lib.ABI_VERSION == 4
 
 
 def test_struct_layouts_match_header():
@@ -37,6 +37,7 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.Fields) == 4 * 8 + 8 + 48
     assert ctypes.sizeof(_lib.State) == 40
     assert ctypes.sizeof(_lib.TrackArgs) == 4 * 8 + 8 + 4 * 8 + 9 * 8
+    assert ctypes.sizeof(_lib.JobDesc) == 40 + ctypes.sizeof(_lib.Fields) + 10 * 8 + 2 * 8
 
 
 def test_capi_argument_errors_without_gpu():
