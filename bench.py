@@ -835,22 +835,26 @@ def main():
         del rh, vh
 
     deposit = electrodes = loader = space_charge = sweep = ring = None
-    if rank == 0 and not args.no_legs:
+    # the single-GPU objects (legs, C2, C5, C4) belong to the one-GPU line; a
+    # multi-GPU (replica) run reports the RF-gap job alone, so the GPUs it
+    # holds are not kept for minutes of work that does not scale
+    single = rank == 0 and world == 1
+    if single and not args.no_legs:
         deposit = run_deposit(d_r0, dev)
         space_charge = run_space_charge(d_r0, dev)
         electrodes = run_electrodes(dev)
         loader = run_loaders(dev)
     del d_r0, d_v0, d_phase
     torch.cuda.empty_cache()
-    if rank == 0 and not args.no_sweep:
+    if single and not args.no_sweep:
         sweep = run_pusher_sweep(dev)
         torch.cuda.empty_cache()
-    if rank == 0 and not args.no_sector_ring:
+    if single and not args.no_sector_ring:
         ring = run_sector_ring(dev)
         torch.cuda.empty_cache()
 
     serving = None
-    if rank == 0 and args.serve_jobs > 0:
+    if single and args.serve_jobs > 0:
         serving = run_serving(args.serve_jobs, dev)
 
     cpu = None
