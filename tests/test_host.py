@@ -69,6 +69,23 @@ def test_capi_argument_errors_without_gpu():
     st = _lib.State(_lib.PREC_F64, 1, 0, None, None, None)
     a.rec_every = 1
     assert lib.ppt_track(st, _lib.Fields(), a, None) == 0
+    # back to row order: a state is needed, then order and scratch
+    assert lib.ppt_restore_order(None, None, None, None, None) == -1
+    assert lib.ppt_restore_order(st, None, None, None, None) == 0          # n = 0
+    st10 = _lib.State(_lib.PREC_F64, 1, 10, 256, None, None)               # never dereferenced here
+    assert lib.ppt_restore_order(st10, None, None, None, None) == -1
+    assert b"order and scratch" in lib.ppt_last_error()
+    # a job's own step window must be in [0, 2^31)
+    job = _lib.JobDesc()
+    job.state = st10
+    job.nsteps_total = 100
+    job.rec_every = 10
+    job.dt = 1e-11
+    job.q_over_m = 1.0
+    job.tick_steps = -1
+    h = ctypes.c_void_p()
+    assert lib.ppt_jobs_create((_lib.JobDesc * 1)(job), 1, 256, h, None) == -1
+    assert b"tick_steps" in lib.ppt_last_error() and not h.value
 
 
 def test_map_layout_choice_without_gpu():
