@@ -204,18 +204,35 @@ __global__ void sort_copy_back(int64_t words, const uint32_t* __restrict__ src, 
         dst[i] = src[i];
 }
 
-// Back to row order: slot s goes to position order[s] (order is a
-// permutation of 0 .. n-1, kept so by the sorts), every state column and the
-// RF phase with it.  A value outside [0, n) is skipped rather than written.
-__global__ void restore_scatter(int64_t n, const int64_t* __restrict__ order, int ncols64,
-                                const double* __restrict__ src64, double* __restrict__ dst64, int na,
-                                const uint32_t* __restrict__ src_a, int nb, const uint32_t* __restrict__ src_b,
-                                uint32_t* __restrict__ dst32, const double* __restrict__ phase,
-                                double* __restrict__ phase_out) {
+// Back to row order: position d takes the slot s with order[s] = d.  First
+// the inverse, perm[order[s]] = s (order is a permutation of 0 .. n-1, kept
+// so by the sorts; a value outside [0, n) is skipped), then a gather that
+// reads the slots scattered and writes every column in order: for the cell
+// order of a bunch that has crossed its map, 2.8 ms against 6.8 ms for the
+// scatter (slot s written to position order[s]) at 1e7 mixed-form particles.
+// (The cell sort keeps its scatter: for the random order of a fresh bunch the
+// gather took 4.5 ms against 2.4 ms.)
+__global__ void restore_inverse(int64_t n, const int64_t* __restrict__ order, uint32_t* __restrict__ perm) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= n) return;
     const int64_t d = order[s];
-    if (d < 0 || d >= n) return;
+    if (d >= 0 && d < n) perm[d] = (uint32_t)s;
+}
+
+// Position d of the permuted copy takes slot perm[d]: ncols64 columns of
+// 8-byte words and na + nb columns of 4-byte words from two sources (mixed
+// state: the int32 cells, then the float32 columns) into one destination
+// block, and the RF phase.  perm values outside [0, n) (positions no slot
+// claimed; none for a permutation) leave position d unwritten.
+__global__ void restore_gather(int64_t n, const uint32_t* __restrict__ perm, int ncols64,
+                               const double* __restrict__ src64, double* __restrict__ dst64, int na,
+                               const uint32_t* __restrict__ src_a, int nb, const uint32_t* __restrict__ src_b,
+                               uint32_t* __restrict__ dst32, const double* __restrict__ phase,
+                               double* __restrict__ phase_out) {
+    const int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const uint32_t s = perm[d];
+    if ((int64_t)s >= n) return;
     for (int c = 0; c < ncols64; ++c) dst64[c * n + d] = src64[c * n + s];
     for (int c = 0; c < na; ++c) dst32[c * n + d] = src_a[c * n + s];
     for (int c = 0; c < nb; ++c) dst32[(na + c) * n + d] = src_b[c * n + s];
@@ -230,7 +247,7 @@ __global__ void iota_rows(int64_t n, int64_t* __restrict__ order) {
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct SortLayout {
-    size_t key, count, tiles, ctrl, tmp64, tmp32, order, phase, total;
+    size_t key, count, tiles, ctrl, tmp64, tmp32, order, phase, perm, total;
 };
 
 static SortLayout sort_layout(int64_t n) {
@@ -245,6 +262,7 @@ static SortLayout sort_layout(int64_t n) {
     L.tmp32 = o; o += align256((size_t)n * 15 * 4);    // mixed: 3 int32 + 12 float32 columns
     L.order = o; o += align256((size_t)n * 8);
     L.phase = o; o += align256((size_t)n * 8);
+    L.perm = o;  o += align256((size_t)n * 4);    // restore: the inverse of order
     L.total = o;
     return L;
 }
@@ -346,15 +364,18 @@ extern "C" int ppt_restore_order(ppt_state* st, int64_t* order, double* rf_phase
     double* tmp64 = reinterpret_cast<double*>(base + L.tmp64);
     uint32_t* tmp32 = reinterpret_cast<uint32_t*>(base + L.tmp32);
     double* phase_tmp = reinterpret_cast<double*>(base + L.phase);
+    uint32_t* perm = reinterpret_cast<uint32_t*>(base + L.perm);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int block = 256;
+    PPT_CUDA_TRY(cudaMemsetAsync(perm, 0xff, (size_t)n * 4, s));   // unclaimed positions: skipped
+    restore_inverse<<<grid_for(n, block), block, 0, s>>>(n, order, perm);
     if (st->precision == PPT_PREC_F64) {
-        restore_scatter<<<grid_for(n, block), block, 0, s>>>(n, order, 6, st->f64, tmp64, 0, nullptr, 0, nullptr,
-                                                             nullptr, rf_phase, phase_tmp);
+        restore_gather<<<grid_for(n, block), block, 0, s>>>(n, perm, 6, st->f64, tmp64, 0, nullptr, 0, nullptr,
+                                                            nullptr, rf_phase, phase_tmp);
         PPT_CUDA_TRY(cudaMemcpyAsync(st->f64, tmp64, (size_t)n * 6 * 8, cudaMemcpyDeviceToDevice, s));
     } else {
-        restore_scatter<<<grid_for(n, block), block, 0, s>>>(
-            n, order, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 12,
+        restore_gather<<<grid_for(n, block), block, 0, s>>>(
+            n, perm, 0, nullptr, nullptr, 3, reinterpret_cast<const uint32_t*>(st->i32), 12,
             reinterpret_cast<const uint32_t*>(st->f32), tmp32, rf_phase, phase_tmp);
         PPT_CUDA_TRY(cudaMemcpyAsync(st->i32, tmp32, (size_t)n * 3 * 4, cudaMemcpyDeviceToDevice, s));
         PPT_CUDA_TRY(cudaMemcpyAsync(st->f32, tmp32 + 3 * n, (size_t)n * 12 * 4, cudaMemcpyDeviceToDevice, s));

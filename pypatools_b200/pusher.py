@@ -337,8 +337,8 @@ class DeviceTracker:
                                               self.rf_phase.data_ptr() if self.rf_phase is not None else None,
                                               scratch.data_ptr(), self._stream(stream)))
         self.row_order = True
-        # scatter, one iota kernel (the copy-backs are memcpy calls)
-        self.launches += 2
+        # inverse, gather and iota kernels (the fill and copy-backs are memset / memcpy calls)
+        self.launches += 3
 
     def sort(self, stream=None):
         """Reorder particles by cell (gather locality)."""
