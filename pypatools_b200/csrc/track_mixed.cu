@@ -4,13 +4,16 @@
 // (Boris pusher.py:124-165, Vay 'vay_rel' :216-279, RK4 :803-892, leapfrog
 // :730-739, record indices :966-1007, fill 0 outside the map
 // interpolators.py:93-97), with:
-//   * positions as int32 cell + float32 in-cell offset (the offset is the
-//     trilinear weight: no per-step cell search),
-//   * float32 node records (128-bit loads), float32 interpolation and
-//     float32 rotation, computing the velocity INCREMENT of the step,
+//   * positions as int32 cell + in-cell offset, the offset a float32 pair
+//     whose high word is the trilinear weight (no per-step cell search) and
+//     moves by exact quanta (add_cells_q, drift_quanta),
+//   * float32 node records (one vector load per corner), float32
+//     interpolation and float32 rotation, computing the velocity INCREMENT
+//     of the step, the E path's roundings kept in low words,
 //   * velocity state as a float32 hi/lo pair updated by an error-free sum,
-//   * float64 only for the field time t_n = t0 + n dt and the RF phase
-//     omega t + phi, reduced to [-pi, pi] before the float32 cosine.
+//   * float64 for the RF factor cos(omega t + phi) (a per-particle phasor
+//     times a per-step table, on the FP64 pipe this kernel otherwise leaves
+//     idle) and for the field time of RK4 stages.
 #include <cmath>
 
 #include "track_params.cuh"
@@ -25,9 +28,8 @@ struct MixCtx {
     const TrackMixDev* P;
     double phase;            // omega t0 + phi_i
     unsigned hits;
-    float c0h, c0l;          // cos of the phase as a float pair
-    float s0h, s0l;          // sin of the phase as a float pair
-    const float4* tab;       // (cos, sin, their low parts) of g omega dt for every g of the launch, or NULL
+    double c0, s0;           // cos and sin of the phase
+    const double2* tab;      // (cos, sin) of g omega dt for every g of the launch, or NULL
     int64_t tab0;            // the launch's first step
 };
 
@@ -41,44 +43,27 @@ __device__ __forceinline__ void rf_turn(int64_t g, double wdt, double& cg, doubl
     sincos((double)g * wdt, &sg, &cg);
 }
 
-// A float64 value as a float pair (head, rest).
-__device__ __forceinline__ float2 split_d(double x) {
-    const float h = (float)x;
-    return make_float2(h, (float)(x - (double)h));
-}
-
-// (cos, sin) of g omega dt and their low parts, from float64
-__device__ __forceinline__ float4 rf_turn_pair(int64_t g, double wdt) {
+// (cos, sin) of g omega dt in float64
+__device__ __forceinline__ double2 rf_turn2(int64_t g, double wdt) {
     double cg, sg;
     rf_turn(g, wdt, cg, sg);
-    const float2 c = split_d(cg), s = split_d(sg);
-    return make_float4(c.x, s.x, c.y, s.y);
+    return make_double2(cg, sg);
 }
 
-// cos(omega (t0 + g dt) + phi_i) = cos(a + b) = cos a cos b - sin a sin b
-// with a = omega t0 + phi_i per particle and b = g omega dt per step, as a
-// float pair good to ~1e-13: both angles' cosines and sines are formed in
-// float64 and kept as float pairs, the two products split exactly (FMA) and
-// their difference by Knuth's two-sum.  A float32 factor would round at
-// 2.8e-8 rms per step, which the E kick carries into every velocity.  The
-// value depends on g and the particle only, table or not, so tracks split
-// into launches differently agree bit for bit.  A launch's table covers every
-// step it evaluates (step0 .. step0 + nsteps).
-__device__ __forceinline__ float2 rf_cos(const MixCtx& c, int64_t g) {
-    const float4 t = c.tab != nullptr ? c.tab[(int)(g - c.tab0)] : rf_turn_pair(g, c.P->wdt);
-    const float p = c.c0h * t.x, pe = fmaf(c.c0h, t.x, -p);
-    const float q = c.s0h * t.y, qe = fmaf(c.s0h, t.y, -q);
-    const float h = p - q;
-    const float bb = h - p;
-    const float err = (p - (h - bb)) + (-q - bb);
-    const float lo = (err + (pe - qe)) + (fmaf(c.c0h, t.z, c.c0l * t.x) - fmaf(c.s0h, t.w, c.s0l * t.y));
-    return make_float2(h, lo);
+// cos(omega (t0 + g dt) + phi_i) = cos a cos b - sin a sin b with a = omega
+// t0 + phi_i per particle and b = g omega dt per step, in float64 (one
+// product and one FMA on the FP64 pipe, which this float32 kernel leaves
+// idle).  The value depends on g and the particle only, table or not, so
+// tracks split into launches differently agree bit for bit.
+__device__ __forceinline__ double rf_cos(const MixCtx& c, int64_t g) {
+    const double2 t = c.tab != nullptr ? c.tab[(int)(g - c.tab0)] : rf_turn2(g, c.P->wdt);
+    return fma(c.c0, t.x, -(c.s0 * t.y));
 }
 
 // Fill the block's RF table for steps step0 .. step0 + n - 1 (all threads
 // of the block call it; n <= kRfTable).
-__device__ __forceinline__ void build_rf_table(float4* tab, int64_t step0, int n, double wdt) {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) tab[i] = rf_turn_pair(step0 + i, wdt);
+__device__ __forceinline__ void build_rf_table(double2* tab, int64_t step0, int n, double wdt) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) tab[i] = rf_turn2(step0 + i, wdt);
     __syncthreads();
 }
 
@@ -261,11 +246,11 @@ __device__ __forceinline__ bool const_fields(const TrackMixDev& P) {
 
 // Fields at the step's field time t0 + g dt (+ toff for RK4 stages); the
 // float64 time and phase are formed only when E is non-zero.
-// (head, tail) of (ch + cl)(eh + el), the product split exactly
-__device__ __forceinline__ void mul_pair(float ch, float cl, float& eh, float& el) {
-    const float h = ch * eh;
-    el = fmaf(ch, eh, -h) + fmaf(ch, el, cl * eh);
-    eh = h;
+// (head, tail) of cf (eh + el), formed in float64 and split
+__device__ __forceinline__ void mul_pair(double cf, float& eh, float& el) {
+    const double e = fma((double)el, cf, (double)eh * cf);
+    eh = (float)e;
+    el = (float)(e - (double)eh);
 }
 
 // El: the low parts of E's components (the interpolation's last level and,
@@ -279,7 +264,7 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
         constexpr int EM = e_bits(L);
         if ((bit(EM, 0) && E.x != 0.0f) || (bit(EM, 1) && E.y != 0.0f) || (bit(EM, 2) && E.z != 0.0f)) {
             // omega (t0 + g dt + toff) + phi_i = (omega t0 + phi_i) + g (omega dt) + omega toff, in float64
-            float2 cf;
+            double cf;
             if (toff == 0.0) {
                 cf = rf_cos(c, g);
             } else {
@@ -289,11 +274,11 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
                 double ph = fma((double)g, c.P->wdt, c.phase);
                 ph = fma(c.P->omega, toff, ph);
                 const double red = fma(-rint(ph * kInvTwoPi), kTwoPi, ph);
-                cf = make_float2(cosf((float)red), 0.0f);
+                cf = (double)cosf((float)red);
             }
-            if constexpr (bit(EM, 0)) mul_pair(cf.x, cf.y, E.x, El.x);
-            if constexpr (bit(EM, 1)) mul_pair(cf.x, cf.y, E.y, El.y);
-            if constexpr (bit(EM, 2)) mul_pair(cf.x, cf.y, E.z, El.z);
+            if constexpr (bit(EM, 0)) mul_pair(cf, E.x, El.x);
+            if constexpr (bit(EM, 1)) mul_pair(cf, E.y, El.y);
+            if constexpr (bit(EM, 2)) mul_pair(cf, E.z, El.z);
         }
     }
     return in || const_fields<L>(*c.P);
@@ -1088,13 +1073,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
         const int64_t row = P.order ? P.order[s] : s;
         if (RF) {
             c.phase = fma(P.omega, P.t0, P.rf_phase[s]);   // omega t0 + phi_i
-            double sa, ca;
-            sincos(c.phase, &sa, &ca);
-            const float2 cp = split_d(ca), sp = split_d(sa);
-            c.c0h = cp.x;
-            c.c0l = cp.y;
-            c.s0h = sp.x;
-            c.s0l = sp.y;
+            sincos(c.phase, &c.s0, &c.c0);
         }
         if (P.flags & PPT_TRACK_INIT) {
             if constexpr (ALG == PPT_ALG_BORIS) {
@@ -1254,9 +1233,9 @@ template <int ALG, bool RF, int L>
 __global__ void __launch_bounds__(128) track_mixed_kernel(const __grid_constant__ TrackMixDev P) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
+    MixCtx c{&P, 0.0, 0u, 0.0, 0.0, nullptr, 0};
     if constexpr (RF) {
-        extern __shared__ float4 rf_tab[];
+        extern __shared__ double2 rf_tab[];
         if (P.rf_tab_n > 0) {
             build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
             c.tab = rf_tab;
@@ -1273,9 +1252,9 @@ __global__ void __launch_bounds__(128) track_mixed_coll_kernel(const __grid_cons
                                                                const __grid_constant__ CollDev C) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     unsigned steps_done = 0;
-    MixCtx c{&P, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
+    MixCtx c{&P, 0.0, 0u, 0.0, 0.0, nullptr, 0};
     if constexpr (RF) {
-        extern __shared__ float4 rf_tab[];
+        extern __shared__ double2 rf_tab[];
         if (P.rf_tab_n > 0) {
             build_rf_table(rf_tab, P.step0, P.rf_tab_n, P.wdt);
             c.tab = rf_tab;
@@ -1317,12 +1296,12 @@ __global__ void __launch_bounds__(kJobBlock) track_mixed_jobs_kernel(const __gri
         __syncthreads();
         if (sP.flags >= 0) {
             const int64_t s = (int64_t)(it - Q.item_start[cj]) * blockDim.x + threadIdx.x;
-            MixCtx c{&sP, 0.0, 0u, 0.0f, 0.0f, 0.0f, 0.0f, nullptr, 0};
+            MixCtx c{&sP, 0.0, 0u, 0.0, 0.0, nullptr, 0};
             if constexpr (RF) {
                 // this job's step window, when the launch reserved a table
                 // that long for it (chunk + 1 entries; a job with a longer
                 // window of its own computes the same values directly)
-                extern __shared__ float4 rf_tab[];
+                extern __shared__ double2 rf_tab[];
                 const int nt = (int)sP.nsteps + 1;
                 if (Q.chunk + 1 <= kRfTable && nt <= Q.chunk + 1) {
                     build_rf_table(rf_tab, sP.step0, nt, sP.wdt);
@@ -1347,11 +1326,11 @@ static cudaError_t launch_mixed_layout(const TrackMixDev* P, const JobQueueDev* 
     if (P) {
         const int block = pick_block(P->n);
         const int g = grid_for(P->n, block);
-        const size_t smem = (size_t)P->rf_tab_n * sizeof(float4);
+        const size_t smem = (size_t)P->rf_tab_n * sizeof(double2);
         if (rf && kE) track_mixed_kernel<ALG, kE, L><<<g, block, smem, s>>>(*P);
         else track_mixed_kernel<ALG, false, L><<<g, block, 0, s>>>(*P);
     } else {
-        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(float4) : 0;
+        const size_t smem = Q->chunk + 1 <= kRfTable ? (size_t)(Q->chunk + 1) * sizeof(double2) : 0;
         if (rf && kE) track_mixed_jobs_kernel<ALG, kE, L><<<grid, kJobBlock, smem, s>>>(*Q);
         else track_mixed_jobs_kernel<ALG, false, L><<<grid, kJobBlock, 0, s>>>(*Q);
     }
@@ -1403,7 +1382,7 @@ static cudaError_t launch_coll_layout(const TrackMixDev& P, const CollDev& C, bo
     constexpr bool kE = layout_has_e(L);
     const int block = pick_block(P.n);
     const int g = grid_for(P.n, block);
-    if (rf && kE) track_mixed_coll_kernel<kE, L><<<g, block, (size_t)P.rf_tab_n * sizeof(float4), s>>>(P, C);
+    if (rf && kE) track_mixed_coll_kernel<kE, L><<<g, block, (size_t)P.rf_tab_n * sizeof(double2), s>>>(P, C);
     else track_mixed_coll_kernel<false, L><<<g, block, 0, s>>>(P, C);
     return cudaGetLastError();
 }
