@@ -814,10 +814,13 @@ def main():
         for _ in range(1):
             pusher.track_batch(wl.r0, wl.v0, efield, bfield, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
         torch.cuda.synchronize()
+        barrier()
         t = time.perf_counter()
         for _ in range(args.e2e_steps):
             rh, vh, _ = pusher.track_batch(wl.r0, wl.v0, efield, bfield, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
-        dt_e2e = time.perf_counter() - t
+        # results are on the host when track_batch returns; the job is done
+        # when the slowest replica's are
+        dt_e2e = max_over_ranks(time.perf_counter() - t, world, dev)
         n_rec = wl.nsteps // wl.rec_every + 1
         # per step: r0 and v0 (n,3) float64 plus the n RF phases in; both
         # (n_rec, n, 3) float64 histories out
