@@ -32,7 +32,7 @@ import numpy as np
 
 from . import _lib
 from .device_fields import FieldCache
-from .pusher import DeviceTracker, _torch
+from .pusher import DeviceTracker, HostStager, _torch, host_array
 
 
 class TrackingJob:
@@ -112,7 +112,6 @@ class TrackingServer:
         self.fields = FieldCache(capacity=16)
         self.compute = torch.cuda.Stream(device=self.device)
         self.upload = torch.cuda.Stream(device=self.device)
-        self.copy = torch.cuda.Stream(device=self.device)
         self.active = []
         self.used_bytes = 0
         self._handle = None
@@ -246,14 +245,20 @@ class TrackingServer:
     # -- retirement ------------------------------------------------------------
     def _collect(self, job, t_base):
         """Start copying a finished job's histories to the host on a worker
-        thread (copy stream), so the loop keeps issuing ticks meanwhile."""
-        torch = self.torch
+        thread, so the loop keeps issuing ticks meanwhile.  The copies go
+        through the device's pinned ring (HostStager): a device-to-pageable
+        copy runs at a few GB/s, the ring at the link's rate.  The job's last
+        tick has completed (the loop synchronised on it), so the copies need
+        no event."""
         tr = job._tracker
+        stager = HostStager.for_device(self.device)
 
         def work():
-            with torch.cuda.device(self.device), torch.cuda.stream(self.copy):
-                r = tr.r_hist.cpu().numpy()
-                v = tr.v_hist.cpu().numpy()
+            r = host_array(tuple(tr.r_hist.shape))
+            v = host_array(tuple(tr.v_hist.shape))
+            stager.copy(tr.r_hist, r)
+            stager.copy(tr.v_hist, v)
+            stager.finish()
             return r, v, time.perf_counter() - t_base
 
         return self._pool.submit(work)
@@ -293,7 +298,7 @@ class TrackingServer:
             # 1) enqueue this tick for the current job set
             ticked = False
             if self.active:
-                # capture only with no result copy in flight: a capture forbids pageable copies in any thread
+                # capture only with no result copy in flight: no other thread syncs on the device then
                 if self.use_graphs and self._graph is None and stable >= self.capture_after and not collecting:
                     self._capture()
                 ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
