@@ -863,7 +863,7 @@ def main():
     cpu = None
     if rank == 0:
         from oracle import cpu_baseline
-        cpu = cpu_baseline.sample(n_sample=20_000, steps=20)
+        cpu = cpu_baseline.sample(n_sample=1_000_000, steps=200)    # ~10 s of CPU work on the host
         cpu["in_map_fraction_gpu_counters"] = roofline["in_map_fraction"]
 
     if rank == 0:

@@ -167,7 +167,7 @@ def run_reference_arm(metric, config, steps, warmup):
     all host threads.  Each bench step is a bounded sample of the RF-gap job
     with the job's phase mix (``blended_sample``); ``metric`` and ``config``
     are the GPU arm's, so the two lines describe the same workload."""
-    n_sample, window = 20_000, 20
+    n_sample, window = 200_000, 50     # ~0.5 s of work per bench step on 16 host threads
     f = in_map_fraction()
     for _ in range(max(1, warmup)):
         blended_sample(2000, 2, f)
