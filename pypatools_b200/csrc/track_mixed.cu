@@ -122,8 +122,11 @@ __device__ __forceinline__ float2 tri8_pair_ff(const float2 q[8], float2 tx, flo
 // El: the low parts of E's components (tri8_pair_ff).
 // fl: the offset's low words (zeros where only the high words are known).
 template <int L>
-__device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3],
-                                             const float fl[3], F3& E, F3& B, F3& El) {
+__device__ __forceinline__ void gather_cell(const TrackMixDev& P, int i, int j, int k, float tx, float ty, float tz,
+                                            F3& E, F3& B, F3& El);
+
+template <int L>
+__device__ __forceinline__ void field_init(const TrackMixDev& P, F3& E, F3& B, F3& El) {
     El = f3(0.0f, 0.0f, 0.0f);
     if constexpr (L == kLayFull) {
         E = f3(P.e_const[0], P.e_const[1], P.e_const[2]);
@@ -132,11 +135,26 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
         E = f3(0.0f, 0.0f, 0.0f);
         B = f3(0.0f, 0.0f, 0.0f);
     }
+}
+
+template <int L>
+__device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cell[3], const float f[3],
+                                             const float fl[3], F3& E, F3& B, F3& El) {
+    field_init<L>(P, E, B, El);
     int i, j, k;
     float tx, ty, tz;
     if (!mixed_axis(cell[0], f[0], fl[0], P.G.n[0], i, tx)) return false;
     if (!mixed_axis(cell[1], f[1], fl[1], P.G.n[1], j, ty)) return false;
     if (!mixed_axis(cell[2], f[2], fl[2], P.G.n[2], k, tz)) return false;
+    gather_cell<L>(P, i, j, k, tx, ty, tz, E, B, El);
+    return true;
+}
+
+// The trilinear fields of cell (i, j, k) at weights (tx, ty, tz), added to
+// the E, B field_init set.
+template <int L>
+__device__ __forceinline__ void gather_cell(const TrackMixDev& P, int i, int j, int k, float tx, float ty, float tz,
+                                            F3& E, F3& B, F3& El) {
     const MapDev& m = P.map;
     const float2 tx2 = make_float2(tx, tx), ty2 = make_float2(ty, ty), tz2 = make_float2(tz, tz);
     constexpr int W = layout_width(L);
@@ -234,7 +252,6 @@ __device__ __forceinline__ bool gather_mixed(const TrackMixDev& P, const int cel
         }
         B = f3(0.0f, 0.0f, tri8([&](int c) { return q[c]; }, tx, ty, tz));
     }
-    return true;
 }
 
 // Constant field parts exist only with the six-component layout.
@@ -256,10 +273,22 @@ __device__ __forceinline__ void mul_pair(double cf, float& eh, float& el) {
 // El: the low parts of E's components (the interpolation's last level and,
 // with RF, the factor's and the product's), for the Boris kick correction.
 template <bool RF, int L>
+__device__ __forceinline__ void rf_modulate(MixCtx& c, int64_t g, double toff, F3& E, F3& El);
+
+template <bool RF, int L>
 __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const float f[3], const float fl[3],
                                              int64_t g, double toff, F3& E, F3& B, F3& El) {
     bool in = gather_mixed<L>(*c.P, cell, f, fl, E, B, El);
     c.hits += in;
+    rf_modulate<RF, L>(c, g, toff, E, El);
+    return in || const_fields<L>(*c.P);
+}
+
+// E times the RF factor at the step's field time t0 + g dt (+ toff), the
+// products' roundings into El; the float64 time and phase are formed only
+// when E is non-zero.
+template <bool RF, int L>
+__device__ __forceinline__ void rf_modulate(MixCtx& c, int64_t g, double toff, F3& E, F3& El) {
     if (RF) {
         constexpr int EM = e_bits(L);
         if ((bit(EM, 0) && E.x != 0.0f) || (bit(EM, 1) && E.y != 0.0f) || (bit(EM, 2) && E.z != 0.0f)) {
@@ -281,7 +310,6 @@ __device__ __forceinline__ bool fields_mixed(MixCtx& c, const int cell[3], const
             if constexpr (bit(EM, 2)) mul_pair(cf, E.z, El.z);
         }
     }
-    return in || const_fields<L>(*c.P);
 }
 
 // The same without the low parts (the pushers other than the Boris family's).
@@ -903,15 +931,34 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float2 o[3], 
     // after field-free runs and steps (normalise), and in the loaded state
     const float cn[3] = {cf[0], cf[1], cf[2]};
     const float fn[3] = {o[0].x, o[1].x, o[2].x};
-    // cheap pre-test on the cell range (the last node layer included); the
-    // exact bounds rule is applied inside gather_mixed
-    const bool maybe = (cn[0] >= 0.0f) & (cn[0] <= P.cell_max[0]) & (cn[1] >= 0.0f) & (cn[1] <= P.cell_max[1]) &
-                       (cn[2] >= 0.0f) & (cn[2] <= P.cell_max[2]);
+    // a cell whose 8 corners are inner nodes on every axis (cells 1 .. n-3):
+    // the offset in [0, 1] keeps the position strictly inside, so the
+    // weights are the offsets, with no face rule to apply; otherwise the
+    // cheap pre-test on the cell range (the last node layer included) and
+    // the exact bounds rule in gather_mixed
+    // (the Boris kernel only: with the relativistic pushers' longer step the
+    // second gather path cost more registers than it saved, 6-7 % slower)
+    const int cell[3] = {(int)cn[0], (int)cn[1], (int)cn[2]};
+    const bool inner = ALG == PPT_ALG_BORIS &&
+                       ((unsigned)(cell[0] - 1) < (unsigned)(P.G.n[0] > 3 ? P.G.n[0] - 3 : 0)) &
+                       ((unsigned)(cell[1] - 1) < (unsigned)(P.G.n[1] > 3 ? P.G.n[1] - 3 : 0)) &
+                       ((unsigned)(cell[2] - 1) < (unsigned)(P.G.n[2] > 3 ? P.G.n[2] - 3 : 0));
+    const bool maybe = inner || ((cn[0] >= 0.0f) & (cn[0] <= P.cell_max[0]) & (cn[1] >= 0.0f) &
+                                 (cn[1] <= P.cell_max[1]) & (cn[2] >= 0.0f) & (cn[2] <= P.cell_max[2]));
     if (maybe || const_fields<L>(P)) {
-        const int cell[3] = {(int)cn[0], (int)cn[1], (int)cn[2]};
         F3 E, B, El;
         const float fln[3] = {o[0].y, o[1].y, o[2].y};
-        if (fields_mixed<RF, L>(c, cell, fn, fln, g, 0.0, E, B, El)) {
+        bool have;
+        if (ALG == PPT_ALG_BORIS && inner) {
+            field_init<L>(P, E, B, El);
+            gather_cell<L>(P, cell[0], cell[1], cell[2], fn[0], fn[1], fn[2], E, B, El);
+            c.hits += 1u;
+            rf_modulate<RF, L>(c, g, 0.0, E, El);
+            have = true;
+        } else {
+            have = fields_mixed<RF, L>(c, cell, fn, fln, g, 0.0, E, B, El);
+        }
+        if (have) {
             F3 v = f3(vh[0], vh[1], vh[2]);
             if constexpr (ALG == PPT_ALG_BORIS) {
                 // only the velocity components the layout's fields can change;
