@@ -856,20 +856,38 @@ __device__ __forceinline__ void normalise(float cf[3], float2 o[3]) {
     }
 }
 
-// m field-free steps from global step g0.  Inside whole carry periods the
-// high words take q at every step -- x and y as one packed FADD2, so a step
-// is two issue slots -- and the low words kCarry r at the carry point (exact,
-// so the same bits as r at every step, see drift_quanta).
+// m field-free steps from global step g0.  The high words take q at every
+// step -- x and y as one packed FADD2, so a step is two issue slots -- and
+// the low words k r at once for the k steps before each carry point and for
+// the steps after the last one (exact, so the same bits as r at every step,
+// see drift_quanta).
 __device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const float2 Q[3], const float2 U[3],
                                             int64_t g0, int m) {
     drift_enter(o, U);
-    int j = 0;
-    for (; j < m && ((unsigned)(g0 + j) & kCarryMask) != 0u; ++j) {
-        add_quanta(o, Q);
-        if (((unsigned)(g0 + j + 1) & kCarryMask) == 0u) carry(cf, o, U);
-    }
     const float2 qxy = make_float2(Q[0].x, Q[1].x);
     const float qz = Q[2].x;
+    // k steps of the high words, k r into the low words
+    auto run = [&](int k) {
+        float2 hxy = make_float2(o[0].x, o[1].x);
+        float hz = o[2].x;
+        for (int i = 0; i < k; ++i) {
+            hxy = __fadd2_rn(hxy, qxy);
+            hz += qz;
+        }
+        o[0].x = hxy.x;
+        o[1].x = hxy.y;
+        o[2].x = hz;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) o[a].y = fmaf((float)k, Q[a].y, o[a].y);
+    };
+    // up to the first carry point (the steps g with (g + 1) % kCarry == 0)
+    const int head = (int)((kCarry - ((unsigned)g0 & kCarryMask)) & kCarryMask);
+    int j = 0;
+    if (head > 0) {
+        j = head < m ? head : m;
+        run(j);
+        if (j == head) carry(cf, o, U);
+    }
     for (; j + kCarry <= m; j += kCarry) {
         float2 hxy = make_float2(o[0].x, o[1].x);
         float hz = o[2].x;
@@ -885,7 +903,7 @@ __device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const floa
         for (int a = 0; a < 3; ++a) o[a].y = fmaf((float)kCarry, Q[a].y, o[a].y);
         carry(cf, o, U);
     }
-    for (; j < m; ++j) add_quanta(o, Q);   // fewer than kCarry steps from an aligned start: no carry point
+    if (j < m) run(m - j);   // fewer than kCarry steps from an aligned start: no carry point
     normalise(cf, o);
 }
 
