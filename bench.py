@@ -145,11 +145,34 @@ def run_pusher_sweep(dev, n=1_000_000, nsteps=10_000, sort_every=100):
         out[alg] = res
         del hist
         torch.cuda.empty_cache()
+    cpu = _sweep_cpu_baseline(wl)
+    for alg, rate in cpu["particle_steps_per_s"].items():
+        out[alg]["cpu_port_particle_steps_per_s"] = rate
     return {"metric": "particle-steps/s per pusher, mixed vs float64, and the mixed form's error",
             "workload": "radial_e_solenoid_electrons", "particles": wl.n, "steps": wl.nsteps, "dt": wl.dt,
             "map": "129^3 over a 20 cm cube: E radial 1 MV/m at r = 0.1 m, Bz = 0.5 T cos(pi z / 0.2 m)",
             "error_metric": "per particle max over the start and end records of |r - r64| / max(|r64|, 0.1 m)",
-            "sort_every": sort_every, "results": out}
+            "sort_every": sort_every, "cpu_baseline": cpu["describe"], "results": out}
+
+
+def _sweep_cpu_baseline(wl, n_sample=100_000, steps=20):
+    """The C restatement of the reference's three pushers (boris, vay_rel,
+    rk4_rel) on the first n_sample electrons of the sweep, all host threads:
+    the per-pusher CPU baseline."""
+    import time
+    from oracle import cpu_baseline
+    omap, keep = cpu_baseline.make_map(wl.grid, wl.e_values, wl.b_values)
+    r0, v0 = wl.r0[:n_sample], wl.v0[:n_sample]
+    rates = {}
+    for alg in ("boris", "vay_rel", "rk4_rel"):
+        cpu_baseline.track(alg, r0[:64], v0[:64], omap, 2, wl.dt, wl.species.q_over_m, rec=2)
+        t = time.perf_counter()
+        cpu_baseline.track(alg, r0, v0, omap, steps, wl.dt, wl.species.q_over_m, rec=steps)
+        rates[alg] = n_sample * steps / (time.perf_counter() - t)
+    del keep
+    return {"particle_steps_per_s": rates,
+            "describe": {"kind": "port", "cores": int(cpu_baseline.load().oracle_threads()),
+                         "sample": f"{n_sample} electrons x {steps} steps per pusher (the C restatement)"}}
 
 
 def run_phases(dev, n=1_000_000, nsteps=1000, sort_every=0, launches=4):

@@ -75,7 +75,40 @@ def main(n=20_000, steps=20, reps=3):
                       "port_over_reference": t_ref / t_port,
                       "max_abs_position_difference_m": float(np.max(np.abs(r_ref - r_port)))}
     del keep
+    res["electron_sweep"] = electron_sweep(pusher, field, n=max(2000, n // 10), steps=steps, reps=reps)
     print(json.dumps(res))
+
+
+def electron_sweep(pusher, field, n=2000, steps=20, reps=3):
+    """The electron sweep's three reference pushers (boris, vay_rel,
+    rk4_rel) on its bunch and 129^3 map (radial E, solenoid B), reference
+    Numba against the C restatement, the same threads."""
+    from pypatools_b200 import workloads
+    from oracle import cpu_baseline
+    wl = workloads.radial_e_solenoid_electrons(n=n, nsteps=steps)
+    g = {"x": wl.grid[0], "y": wl.grid[1], "z": wl.grid[2]}
+    ef = field.Field.from_arrays(g, {c: np.asarray(wl.e_values[c], dtype=np.float64) for c in "xyz"})
+    bf = field.Field.from_arrays(g, {c: np.asarray(wl.b_values[c], dtype=np.float64) for c in "xyz"})
+    omap, keep = cpu_baseline.make_map(wl.grid, wl.e_values, wl.b_values)
+
+    class Ion:
+        q_over_m = wl.species.q_over_m
+
+    out = {"sample": f"{n} electrons x {steps} steps, 129^3 map (radial E, solenoid B)"}
+    for alg in ("boris", "vay_rel", "rk4_rel"):
+        ref = pusher.Pusher(Ion(), alg, use_numba=True)
+        ref.track_batch(wl.r0[:64], wl.v0[:64], ef, bf, 2, wl.dt, 2)                 # Numba compile
+        t_ref = _best(lambda: ref.track_batch(wl.r0, wl.v0, ef, bf, steps, wl.dt, steps), reps)
+        t_port = _best(lambda: cpu_baseline.track(alg, wl.r0, wl.v0, omap, steps, wl.dt, wl.species.q_over_m,
+                                                   rec=steps), reps)
+        r_ref, _, _ = ref.track_batch(wl.r0, wl.v0, ef, bf, steps, wl.dt, steps)
+        r_port, _ = cpu_baseline.track(alg, wl.r0, wl.v0, omap, steps, wl.dt, wl.species.q_over_m, rec=steps)
+        out[alg] = {"reference_numba_particle_steps_per_s": n * steps / t_ref,
+                    "port_particle_steps_per_s": n * steps / t_port,
+                    "port_over_reference": t_ref / t_port,
+                    "max_abs_position_difference_m": float(np.max(np.abs(r_ref - r_port)))}
+    del keep
+    return out
 
 
 if __name__ == "__main__":
