@@ -6,7 +6,7 @@ the bar is bitwise equality)."""
 import numpy as np
 import pytest
 
-from pypatools_b200 import PusherGPU, Field, IonSpecies, workloads
+from pypatools_b200 import PusherGPU, Field, IonSpecies, RFModulation, workloads
 from pypatools_b200.serving import TrackingJob, TrackingServer
 
 pytestmark = pytest.mark.gpu
@@ -36,7 +36,7 @@ def _jobs(fields, n_jobs=10, spacing=0.002, steps_max=300):
 def _check_alone(ion, jobs):
     for job in jobs:
         rh, vh, _ = PusherGPU(ion, job.algorithm, precision=job.precision).track_batch(
-            job.r0, job.v0, job.efield, job.bfield, job.nsteps, job.dt, job.rec_every)
+            job.r0, job.v0, job.efield, job.bfield, job.nsteps, job.dt, job.rec_every, rf=job.rf)
         np.testing.assert_array_equal(job.r_hist, rh, err_msg=f"job {job.job_id} r")
         np.testing.assert_array_equal(job.v_hist, vh, err_msg=f"job {job.job_id} v")
 
@@ -88,6 +88,12 @@ def test_serving_per_job_windows(cuda):
     of the job run alone, bit for bit."""
     fields = _map_fields()
     ion, jobs = _jobs(fields, n_jobs=8, spacing=0.0)
+    # half of them with an RF-modulated E: their windows (up to 256 steps) are
+    # longer than the tick's RF table (33 entries), so they form the factor
+    # without it -- the same values
+    rng = np.random.default_rng(9)
+    for j in jobs[::2]:
+        j.rf = RFModulation(1e8, rng.uniform(0.0, 2 * np.pi, j.n))
     server = TrackingServer(chunk=32, use_graphs=False, small_bunch=1 << 20, max_boost=8)
     windows = {j.job_id: server._tick_steps(j) for j in jobs}
     assert all(w > 32 for w in windows.values())
