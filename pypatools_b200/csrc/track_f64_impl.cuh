@@ -229,13 +229,24 @@ __device__ __forceinline__ int eval_single_f64(const MapDev& m, V3 r, V3& E, V3&
     const double x[3] = {r.x, r.y, r.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const AxisDev& ax = m.ax[a];
-        const double u = (x[a] - ax.lo) * ax.inv_d;
-        int cc = (int)floor(u);
-        cc = cc < 0 ? 0 : (cc > ax.n - 2 ? ax.n - 2 : cc);
-        const double t = u - (double)cc;
-        tt[a] = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
-        ijk[a] = cc;
+        const double u = (x[a] - m.ax[a].lo) * m.ax[a].inv_d;
+        ijk[a] = __double2int_rd(u);             // floor: u is in [0, n - 1] here
+        tt[a] = u - (double)ijk[a];
+    }
+    // cells 1 .. n-3 on every axis need none of the clamps below (the cell is
+    // in range and u - floor(u) is in [0, 1)); the others take them
+    if (!(((unsigned)(ijk[0] - 1) < (unsigned)(m.ax[0].n - 3)) & ((unsigned)(ijk[1] - 1) < (unsigned)(m.ax[1].n - 3)) &
+          ((unsigned)(ijk[2] - 1) < (unsigned)(m.ax[2].n - 3)))) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const AxisDev& ax = m.ax[a];
+            const double u = (x[a] - ax.lo) * ax.inv_d;
+            int cc = ijk[a];
+            cc = cc < 0 ? 0 : (cc > ax.n - 2 ? ax.n - 2 : cc);
+            const double t = u - (double)cc;
+            tt[a] = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+            ijk[a] = cc;
+        }
     }
     c.tx = tt[0];
     c.ty = tt[1];
