@@ -45,7 +45,8 @@ def parse():
                          "(--n particles, --nsteps steps per drift launch)")
     ap.add_argument("--n", type=int, default=None, help="particles (default: the workload's)")
     ap.add_argument("--nsteps", type=int, default=None, help="steps per job (default: the workload's)")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3,
+                    help="timed track_batch calls of the e2e figure (their mean)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--long-chunk", type=int, default=1000,
@@ -839,7 +840,9 @@ def main():
         torch.cuda.synchronize()
         barrier()
         t = time.perf_counter()
+        rh = vh = None
         for _ in range(args.e2e_steps):
+            rh = vh = None            # a caller that is done with the previous call's results
             rh, vh, _ = pusher.track_batch(wl.r0, wl.v0, efield, bfield, wl.nsteps, wl.dt, wl.rec_every, rf=rf)
         # results are on the host when track_batch returns; the job is done
         # when the slowest replica's are
