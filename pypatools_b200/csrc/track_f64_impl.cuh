@@ -322,6 +322,56 @@ __device__ __forceinline__ V3 drift(V3 r, V3 v, double dt) {
     return v3(fma(v.x, dt, r.x), fma(v.y, dt, r.y), fma(v.z, dt, r.z));
 }
 
+// m field-free steps of one coordinate, x <- fma(v, dt, x) at each, with the
+// bits of the step-by-step loop.  The float64 numbers whose magnitude lies
+// in one binade [2^E, 2^(E+1)) are the multiples of g = 2^(E-52) there, and x
+// is one of them; so when the exact sum x + v dt lies in x's binade it rounds
+// to x + D, D being v dt rounded to a multiple of g -- the same D at every
+// such step, unless v dt lies exactly halfway between two multiples (then
+// round-half-even looks at x's last bit).  Each trip of the loop therefore
+// takes the steps whose sums certainly stay inside x's binade as k D in one
+// exact fused multiply-add, then one step as it comes (the step out of the
+// binade, a halfway case, or a step within four steps of zero).  A
+// coordinate crossing zero passes the binades between |v dt| and |x| one
+// trip each.
+__device__ __forceinline__ double drift_coord(double x, double v, double dt, int m) {
+    // a zero advance: the first step settles the sign of a zero x, the others keep x
+    if (v == 0.0 || dt == 0.0) return m > 0 ? fma(v, dt, x) : x;
+    const double p = v * dt;
+    const double ap = fabs(p) * (1.0 + 0x1p-50);   // above |v dt| exactly
+    while (m > 0) {
+        const double ax = fabs(x);
+        // (false for NaN and infinities too)
+        if (ax >= 4.0 * ap && ax >= 0x1p-64 && ax < 0x1p1000) {
+            const long long eb = __double_as_longlong(ax) >> 52;    // biased exponent of |x|
+            const double lo = __longlong_as_double(eb << 52);        // 2^E
+            const double D = fma(v, dt, x) - x;   // exact: the sum lies within [x/2, 2x]
+            // distance of the sums from the binade's edge ahead, from below
+            const double room = ((p > 0.0) == (x > 0.0) ? 2.0 * lo - ax : ax - lo) - ap;
+            // not halfway: |v dt - D| != g / 2 = 2^(E-53)
+            if (room > 0.0 && fabs(fma(v, dt, -D)) != __longlong_as_double((eb - 53) << 52)) {
+                // steps n = 0 .. k-1 with n |D| < room; the quotient's error
+                // (a few float32 ulps) is far inside the 1e-4 margin
+                int k = m;
+                if (D != 0.0) {
+                    const float kq = __fdividef((float)room, (float)fabs(D)) * 0.9999f;
+                    if (!(kq >= (float)m)) k = kq >= 1.0f ? (int)kq : 1;
+                }
+                x = fma((double)k, D, x);
+                m -= k;
+                if (m == 0) break;
+            }
+        }
+        x = fma(v, dt, x);
+        --m;
+    }
+    return x;
+}
+
+__device__ __forceinline__ V3 drift_run(V3 r, V3 v, double dt, int m) {
+    return v3(drift_coord(r.x, v.x, dt, m), drift_coord(r.y, v.y, dt, m), drift_coord(r.z, v.z, dt, m));
+}
+
 __host__ __device__ constexpr bool alg_skips_free(int a) {
     return a == PPT_ALG_LEAPFROG || a == PPT_ALG_BORIS || a == PPT_ALG_BORIS_REL;
 }
@@ -524,15 +574,7 @@ __device__ __forceinline__ unsigned track_f64_particle(const TrackDev& P, int64_
                     if (quiet > 0) {
                         // a run of field-free steps: the same position advance, no field lookups
                         const int m = quiet < seg - i ? quiet : seg - i;
-                        const V3 v = w_to_v<ALG>(w);
-                        int j = 0;
-                        for (; j + 4 <= m; j += 4) {   // the same per-step advance, four per trip
-                            r = drift(r, v, P.dt);
-                            r = drift(r, v, P.dt);
-                            r = drift(r, v, P.dt);
-                            r = drift(r, v, P.dt);
-                        }
-                        for (; j < m; ++j) r = drift(r, v, P.dt);
+                        r = drift_run(r, w_to_v<ALG>(w), P.dt, m);
                         i += m;
                         quiet -= m;
                     } else {

@@ -6,7 +6,9 @@
 // interpolators.py:93-97), with:
 //   * positions as int32 cell + in-cell offset, the offset a float32 pair
 //     whose high word is the trilinear weight (no per-step cell search) and
-//     moves by exact quanta (add_cells_q, drift_quanta),
+//     moves by exact quanta (add_cells_q, drift_quanta), so that a run of
+//     field-free steps takes O(1) work with the bits of the steps taken one
+//     by one (drift_steps, carry_periods),
 //   * float32 node records (one vector load per corner), float32
 //     interpolation and float32 rotation, computing the velocity INCREMENT
 //     of the step, the E path's roundings kept in low words,
@@ -765,8 +767,9 @@ struct Drift {
 // with no constant field both updates leave v exactly unchanged (every added
 // term is zero), so such a step is the position advance alone.  The offset
 // is a (hi, lo) pair per axis; a field-free step adds the drift quanta (q, r)
-// of the increment (drift_quanta) to it with one packed FADD2, and hi + q is
-// exact, so the drift does not round the position step after step.  The
+// of the increment (drift_quanta) to it, and hi + q is exact, so the drift
+// does not round the position step after step (and drift_steps takes a run
+// of such steps as one multiply-add).  The
 // whole-cell carry is taken after global steps g with (g + 1) % kCarry == 0
 // only; in between hi runs up to 1 + kCarry |dh| cells.  Because the carry
 // points depend on the global step index alone, a track gives the same bits
@@ -781,8 +784,9 @@ constexpr unsigned kCarryMask = kCarry - 1;
 // period reaches (|hi| < 2 + kCarry |dh|); r = (dh - q) + dl the rest,
 // rounded to a multiple of u 2^-19.  Once hi is a multiple of u (after at
 // most a few roundings at the start of a drift), hi + q is exact; and the low
-// word, a multiple of u 2^-19 below 32 u (the carry keeps it below
-// (kCarry + 1) u / 2 = 16.5 u), is changed by exact additions only, so
+// word, a multiple of u 2^-19 below 32 u (after a carry it lies in [0, u),
+// and a period adds at most kCarry |r| <= 16.5 u), changes by exact additions
+// only, so
 // whether r is added at every step or kCarry r at a carry point gives the
 // same bits.  Without the split, the float32 sum hi + dh rounds dh to the
 // spacing of hi's binade, the same amount every step: a fixed-sign error of
@@ -806,18 +810,47 @@ __device__ __forceinline__ void drift_quanta(const Drift& d, float2 Q[3], float2
 }
 
 // The carry of field-free steps: whole cells out of the high word, and the
-// whole quanta the low word has gathered (N r after N steps) into it, so the
-// high word -- which the cell pre-test and the trilinear weight read --
-// stays within u of the position.  Both moves are exact.
+// whole quanta the low word has gathered (N r after N steps) into it, which
+// leaves the low word in [0, u), so the high word -- which the cell pre-test
+// and the trilinear weight read -- stays within u of the position.  Both
+// moves are exact.
 __device__ __forceinline__ void carry(float cf[3], float2 o[3], const float2 U[3]) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float cc = floorf(o[a].x);
         o[a].x -= cc;
         cf[a] += cc;
-        const float qq = rintf(o[a].y * U[a].y) * U[a].x;
+        const float qq = floorf(o[a].y * U[a].y) * U[a].x;
         o[a].x += qq;
         o[a].y -= qq;
+    }
+}
+
+// N whole carry periods (kCarry steps, then the carry) from a carry point,
+// in closed form.  In units of w = u 2^-19 the low word is an integer L and a
+// period's kCarry r an integer R; a carry moves floor((L + R) / 2^19) quanta u
+// into the high word and leaves (L + R) mod 2^19, so after N periods the low
+// word is (L0 + N R) mod 2^19 and the quanta moved sum to
+// floor((L0 + N R) / 2^19).  The cell plus the high word, T, gains kCarry q
+// and the moved quanta each period, and the last carry splits T less its own
+// quanta into the whole cells and the rest.  Every term is a multiple of u
+// below 2^53 u, summed exactly in float64, so the result has the bits of the
+// N periods taken one by one.
+__device__ __forceinline__ void carry_periods(float cf[3], float2 o[3], const float2 Q[3], const float2 U[3],
+                                              int N) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float u = U[a].x, wi = U[a].y * 0x1p19f;
+        const long long L0 = __float2int_rz(o[a].y * wi);               // exact integers below 2^24
+        const long long R = __float2int_rz((float)kCarry * Q[a].y * wi);
+        const long long X = L0 + (long long)N * R;
+        const long long Lp = N >= 2 ? ((X - R) & 0x7ffff) : L0;        // the low word before the last period
+        const double T = ((double)cf[a] + (double)o[a].x) + (double)(kCarry * N) * (double)Q[a].x +
+                         (double)u * (double)(X >> 19);
+        const double cN = floor(T - (double)u * (double)((Lp + R) >> 19));
+        cf[a] = (float)cN;
+        o[a].x = (float)(T - cN);
+        o[a].y = (float)(X & 0x7ffff) * (u * 0x1p-19f);
     }
 }
 
@@ -856,29 +889,26 @@ __device__ __forceinline__ void normalise(float cf[3], float2 o[3]) {
     }
 }
 
-// m field-free steps from global step g0.  The high words take q at every
-// step -- x and y as one packed FADD2, so a step is two issue slots -- and
-// the low words k r at once for the k steps before each carry point and for
-// the steps after the last one (exact, so the same bits as r at every step,
-// see drift_quanta).
+// m field-free steps from global step g0.  Every field-free step adds q to
+// the high words exactly (drift_quanta), so the k steps up to the first carry
+// point, and those after the last, leave hi + k q, which one fused
+// multiply-add yields with its single rounding: the same bits as k additions
+// (x and y as one packed FFMA2).  The low words take k r the same way, and
+// the whole periods in between go in closed form (carry_periods).  The
+// carries stay where the global step index puts them.
 __device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const float2 Q[3], const float2 U[3],
                                             int64_t g0, int m) {
     drift_enter(o, U);
     const float2 qxy = make_float2(Q[0].x, Q[1].x);
     const float qz = Q[2].x;
-    // k steps of the high words, k r into the low words
     auto run = [&](int k) {
-        float2 hxy = make_float2(o[0].x, o[1].x);
-        float hz = o[2].x;
-        for (int i = 0; i < k; ++i) {
-            hxy = __fadd2_rn(hxy, qxy);
-            hz += qz;
-        }
+        const float kf = (float)k;
+        const float2 hxy = __ffma2_rn(make_float2(kf, kf), qxy, make_float2(o[0].x, o[1].x));
         o[0].x = hxy.x;
         o[1].x = hxy.y;
-        o[2].x = hz;
+        o[2].x = fmaf(kf, qz, o[2].x);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) o[a].y = fmaf((float)k, Q[a].y, o[a].y);
+        for (int a = 0; a < 3; ++a) o[a].y = fmaf(kf, Q[a].y, o[a].y);
     };
     // up to the first carry point (the steps g with (g + 1) % kCarry == 0)
     const int head = (int)((kCarry - ((unsigned)g0 & kCarryMask)) & kCarryMask);
@@ -888,20 +918,10 @@ __device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const floa
         run(j);
         if (j == head) carry(cf, o, U);
     }
-    for (; j + kCarry <= m; j += kCarry) {
-        float2 hxy = make_float2(o[0].x, o[1].x);
-        float hz = o[2].x;
-#pragma unroll
-        for (int k = 0; k < kCarry; ++k) {
-            hxy = __fadd2_rn(hxy, qxy);
-            hz += qz;
-        }
-        o[0].x = hxy.x;
-        o[1].x = hxy.y;
-        o[2].x = hz;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) o[a].y = fmaf((float)kCarry, Q[a].y, o[a].y);
-        carry(cf, o, U);
+    const int np = (m - j) / kCarry;
+    if (np > 0) {
+        carry_periods(cf, o, Q, U, np);
+        j += np * kCarry;
     }
     if (j < m) run(m - j);   // fewer than kCarry steps from an aligned start: no carry point
     normalise(cf, o);

@@ -160,3 +160,48 @@ def test_row_order_restored_after_the_bunch_leaves(cuda, precision):
     tr.step = 0
     tr.load(r0, v0)
     assert tr.order is None and not tr.row_order
+
+
+def _fma_exact(a, b, c):
+    """a * b + c rounded once (float64), as the device's fma."""
+    from fractions import Fraction
+    s = Fraction(a) * Fraction(b) + Fraction(c)
+    if s == 0:
+        # an exact zero sum is -0 only when both addends are -0
+        return -0.0 if (np.signbit(a) != np.signbit(b)) and np.signbit(c) else 0.0
+    return float(s)
+
+
+def test_f64_field_free_runs_are_stepwise_fma(cuda):
+    """Outside the maps the float64 kernel takes a run of field-free steps a
+    binade at a time (k D in one fused multiply-add, see drift_coord); the
+    positions must be those of x <- fma(v, dt, x) at every step, bit for bit:
+    coordinates crossing zero (many binades), z through powers of two, zero
+    velocity components, and steps exactly halfway between two float64
+    neighbours (round-half-even alternates)."""
+    rng = np.random.default_rng(5)
+    dt = 2.0 ** -33                      # v dt exact for the halfway cases below
+    nsteps, rec = 2000, 500
+    rows = []
+    for i in range(40):                  # transverse coordinates crossing zero
+        vx, vy = rng.choice([-1, 1], 2) * 10 ** rng.uniform(2, 5, 2)
+        kx, ky = rng.uniform(0, 1500, 2)
+        rows.append(([-vx * dt * kx, -vy * dt * ky, rng.uniform(0.06, 0.4)], [vx, vy, 10 ** rng.uniform(6, 7.3)]))
+    for z in (0.0625, 0.125, 0.25, 0.5, 1.0):   # z starting on a power of two
+        rows.append(([1e-3, -2e-3, z], [3e3, -1e4, 1.2e7]))
+    rows.append(([0.0, -0.0, 0.07], [0.0, 0.0, 1e7]))          # zero velocity components
+    rows.append(([0.75, -0.75, 0.08], [1 + 2.0 ** -21, -(1 + 2.0 ** -21), 1e7]))   # halfway, both signs
+    rows.append(([0.3, 1e-9, 0.09], [(2 ** 18 + 0.5) * 2.0 ** -21, 5.0, 2e6]))     # halfway in [0.25, 0.5)
+    r0 = np.array([r for r, _ in rows], dtype=np.float64)
+    v0 = np.array([v for _, v in rows], dtype=np.float64)
+    rh, vh, _ = PusherGPU(IonSpecies("proton"), "boris").track_batch(r0, v0, Field.zero(3), _uniform_b(1.0, half=0.05),
+                                                                   nsteps, dt, rec)
+    assert np.array_equal(vh[0], v0)     # outside the map: no kick
+    for p in range(len(rows)):
+        for a in range(3):
+            x = float(r0[p, a])
+            for s in range(1, nsteps + 1):
+                x = _fma_exact(float(v0[p, a]), dt, x)
+                if s % rec == 0:
+                    got = float(rh[s // rec, p, a])
+                    assert got == x and np.signbit(got) == np.signbit(x), (p, a, s, got, x)
