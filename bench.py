@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--long-chunk", type=int, default=1000,
                     help="steps per launch once the bunch has left the map (no sorts then)")
+    ap.add_argument("--free-chunk", type=int, default=None,
+                    help="steps per launch once the bunch is back in row order and met no map "
+                         "(default 4 x --long-chunk)")
     ap.add_argument("--sort-every", type=int, default=None,
                     help="cell re-sort interval in steps while the map is populated (also the launch length "
                          "then); 0 = never; default 300 for rf_gap (best of a 50-1000 sweep), 100 otherwise "
@@ -78,11 +81,11 @@ def parse():
 # launch inside the map (the 60 B state read and written; the map's occupied
 # cells stay in L1/L2) and a 1000-step field-free launch (the state and two
 # 48 B snapshot rows).
-MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = {"map": 131.0, "drift": 167.2}
+MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = {"map": 131.0, "drift": 165.9}
 # Warp-instructions issued per warp-step (32 particle-steps) by the mixed
 # Boris kernel on the RF-gap layout, in the map and in field-free drift
 # (ncu smsp__inst_executed of those launches / warps / steps).
-WARP_INST_PER_WARP_STEP = {"map": 213.7, "drift": 4.1}
+WARP_INST_PER_WARP_STEP = {"map": 213.7, "drift": 1.37}
 MIXED_STATE_BYTES = 60
 
 
@@ -698,7 +701,7 @@ def main():
             tr.rf_phase.copy_(d_phase)
             tr.load(d_r0, d_v0)
             tr.run(wl.nsteps, chunk, sort_every=args.sort_every, long_chunk=args.long_chunk,
-                   launch_events=launch_ev if time_launches else None)
+                   free_chunk=args.free_chunk, launch_events=launch_ev if time_launches else None)
 
         for _ in range(args.warmup):
             job(False)

@@ -831,25 +831,30 @@ __device__ __forceinline__ void carry(float cf[3], float2 o[3], const float2 U[3
 // period's kCarry r an integer R; a carry moves floor((L + R) / 2^19) quanta u
 // into the high word and leaves (L + R) mod 2^19, so after N periods the low
 // word is (L0 + N R) mod 2^19 and the quanta moved sum to
-// floor((L0 + N R) / 2^19).  The cell plus the high word, T, gains kCarry q
-// and the moved quanta each period, and the last carry splits T less its own
-// quanta into the whole cells and the rest.  Every term is a multiple of u
-// below 2^53 u, summed exactly in float64, so the result has the bits of the
+// floor((L0 + N R) / 2^19).  In units of u (u = 2^-s) the high word H gains
+// kCarry q / u and the moved quanta each period, and each carry takes the
+// whole cells out of it; so after the last carry the cells moved out are
+// floor((A - Kp) / 2^s), with A the high word's total and Kp the last
+// period's quanta, and the high word keeps the rest of A.  All of it is exact
+// integer arithmetic on exact conversions, so the result has the bits of the
 // N periods taken one by one.
 __device__ __forceinline__ void carry_periods(float cf[3], float2 o[3], const float2 Q[3], const float2 U[3],
                                               int N) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const float u = U[a].x, wi = U[a].y * 0x1p19f;
-        const long long L0 = __float2int_rz(o[a].y * wi);               // exact integers below 2^24
+        const float u = U[a].x, ui = U[a].y, wi = ui * 0x1p19f;
+        const int sh = (__float_as_int(ui) >> 23) - 127;               // ui = 2^sh
+        // exact integers below 2^24 in magnitude
+        const long long H = __float2int_rz(o[a].x * ui);
+        const long long L0 = __float2int_rz(o[a].y * wi);
+        const long long Qi = __float2int_rz(Q[a].x * ui);
         const long long R = __float2int_rz((float)kCarry * Q[a].y * wi);
         const long long X = L0 + (long long)N * R;
         const long long Lp = N >= 2 ? ((X - R) & 0x7ffff) : L0;        // the low word before the last period
-        const double T = ((double)cf[a] + (double)o[a].x) + (double)(kCarry * N) * (double)Q[a].x +
-                         (double)u * (double)(X >> 19);
-        const double cN = floor(T - (double)u * (double)((Lp + R) >> 19));
-        cf[a] = (float)cN;
-        o[a].x = (float)(T - cN);
+        const long long A = H + (long long)(kCarry * N) * Qi + (X >> 19);
+        const long long C = (A - ((Lp + R) >> 19)) >> sh;               // whole cells moved out
+        cf[a] += (float)C;
+        o[a].x = (float)(A - (C << sh)) * u;
         o[a].y = (float)(X & 0x7ffff) * (u * 0x1p-19f);
     }
 }
@@ -896,9 +901,11 @@ __device__ __forceinline__ void normalise(float cf[3], float2 o[3]) {
 // (x and y as one packed FFMA2).  The low words take k r the same way, and
 // the whole periods in between go in closed form (carry_periods).  The
 // carries stay where the global step index puts them.
+// (on_grid: the offset pair is on the drift's grids already, the previous
+// run having left it there, so drift_enter would change nothing.)
 __device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const float2 Q[3], const float2 U[3],
-                                            int64_t g0, int m) {
-    drift_enter(o, U);
+                                            int64_t g0, int m, bool on_grid) {
+    if (!on_grid) drift_enter(o, U);
     const float2 qxy = make_float2(Q[0].x, Q[1].x);
     const float qz = Q[2].x;
     auto run = [&](int k) {
@@ -1186,6 +1193,7 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
             // record-free segments: the inner loop carries only its counter
             int k = 0;
             int quiet = 0;   // upcoming steps known to be field-free (quiet_steps)
+            bool on_grid = false;   // the last steps were a field-free run (drift_steps)
             while (k < nsteps) {
                 const int64_t to_rec = (int64_t)until + 1;
                 const int seg = (int)(to_rec < (int64_t)(nsteps - k) ? to_rec : (int64_t)(nsteps - k));
@@ -1224,11 +1232,13 @@ __device__ __forceinline__ unsigned track_mixed_particle(const TrackMixDev& P, i
                         const int m = quiet < seg - i ? quiet : seg - i;
                         float2 Q[3], U[3];
                         drift_quanta(d, Q, U);
-                        drift_steps(cf, o, Q, U, g0 + i, m);
+                        drift_steps(cf, o, Q, U, g0 + i, m, on_grid);
+                        on_grid = true;
                         i += m;
                         quiet -= m;
                     } else {
                         quiet = family_step<ALG, RF, L>(c, cf, o, vh, vl, d, g0 + i);
+                        on_grid = false;
                         ++i;
                     }
                 }

@@ -234,7 +234,7 @@ class DeviceTracker:
         self.step += k
 
     def run(self, nsteps, chunk, sort_every=0, long_chunk=None, after_launch=None, launch_events=None,
-            stream=None, in_flight=2):
+            stream=None, in_flight=2, free_chunk=None):
         """Advance ``nsteps`` steps in launches of at most ``chunk`` steps.
 
         With ``sort_every`` > 0 and maps present the schedule follows the
@@ -249,7 +249,10 @@ class DeviceTracker:
         launches are queued ahead, so the GPU never waits on the host.
         Once a finished launch met no map at all, the particles go back to
         row order (``restore_order``) for the snapshot rows' sake, until a
-        map holds particles again.
+        map holds particles again; launches in row order with no map met take
+        ``free_chunk`` steps (default 4 ``long_chunk``): their field-free runs
+        cost little, so the state read and written per launch is what a
+        longer launch saves.
         ``after_launch(steps_done)`` runs after each launch is enqueued;
         ``launch_events`` (a list) receives (start event, end event, first
         step, steps) for each track launch."""
@@ -258,6 +261,7 @@ class DeviceTracker:
         chunk = max(1, int(chunk))
         adaptive = sort_every > 0 and self.dfields.has_maps and self.n > 0
         long_chunk = max(chunk, int(long_chunk or 10 * max(sort_every, 1)))
+        free_chunk = max(long_chunk, int(free_chunk or 4 * long_chunk))
         st = torch.cuda.current_stream(self.device) if stream is None else stream
         if adaptive and self.counters is None:
             self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
@@ -291,7 +295,10 @@ class DeviceTracker:
                     sorted_sparse = not dense
                 elif empty and not self.row_order:
                     self.restore_order(stream)
-                k = min(sort_every if dense else long_chunk, chunk if dense else long_chunk, nsteps - done)
+                if dense:
+                    k = min(sort_every, chunk, nsteps - done)
+                else:
+                    k = min(free_chunk if (empty and self.row_order) else long_chunk, nsteps - done)
                 if dense:
                     k = min(k, sort_every - self.step % sort_every)
             else:
