@@ -81,11 +81,11 @@ def parse():
 # launch inside the map (the 60 B state read and written; the map's occupied
 # cells stay in L1/L2) and a 1000-step field-free launch (the state and two
 # 48 B snapshot rows).
-MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = {"map": 131.0, "drift": 165.9}
+MIXED_DRAM_BYTES_PER_PARTICLE_LAUNCH = {"map": 131.0, "drift": 167.4}
 # Warp-instructions issued per warp-step (32 particle-steps) by the mixed
 # Boris kernel on the RF-gap layout, in the map and in field-free drift
 # (ncu smsp__inst_executed of those launches / warps / steps).
-WARP_INST_PER_WARP_STEP = {"map": 213.7, "drift": 1.37}
+WARP_INST_PER_WARP_STEP = {"map": 213.7, "drift": 1.42}
 MIXED_STATE_BYTES = 60
 
 
