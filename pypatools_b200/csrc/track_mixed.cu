@@ -984,10 +984,8 @@ __device__ __forceinline__ int family_step(MixCtx& c, float cf[3], float2 o[3], 
     // (the Boris kernel only: with the relativistic pushers' longer step the
     // second gather path cost more registers than it saved, 6-7 % slower)
     const int cell[3] = {(int)cn[0], (int)cn[1], (int)cn[2]};
-    const bool inner = ALG == PPT_ALG_BORIS &&
-                       ((unsigned)(cell[0] - 1) < (unsigned)(P.G.n[0] > 3 ? P.G.n[0] - 3 : 0)) &
-                       ((unsigned)(cell[1] - 1) < (unsigned)(P.G.n[1] > 3 ? P.G.n[1] - 3 : 0)) &
-                       ((unsigned)(cell[2] - 1) < (unsigned)(P.G.n[2] > 3 ? P.G.n[2] - 3 : 0));
+    const bool inner = ALG == PPT_ALG_BORIS && ((unsigned)(cell[0] - 1) < P.inner_span[0]) &
+                       ((unsigned)(cell[1] - 1) < P.inner_span[1]) & ((unsigned)(cell[2] - 1) < P.inner_span[2]);
     const bool maybe = inner || ((cn[0] >= 0.0f) & (cn[0] <= P.cell_max[0]) & (cn[1] >= 0.0f) &
                                  (cn[1] <= P.cell_max[1]) & (cn[2] >= 0.0f) & (cn[2] <= P.cell_max[2]));
     if (maybe || const_fields<L>(P)) {
@@ -1515,6 +1513,7 @@ int make_track_mixed(const FieldsDev& F, const ppt_state* st, const ppt_track_ar
         P->kl[c] = (float)(k - (double)P->kh[c]);
         P->inv_d[c] = (float)P->G.inv_d[c];
         P->cell_max[c] = (float)(P->G.n[c] - 1);
+        P->inner_span[c] = P->G.n[c] > 3 ? (uint32_t)(P->G.n[c] - 3) : 0u;
     }
     P->const_nz = F.e_const_nz || F.b_const_nz;
     if (P->const_nz && P->map.layout != kLayFull)

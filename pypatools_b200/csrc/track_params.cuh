@@ -69,6 +69,7 @@ struct TrackMixDev {
     int32_t rf_tab_n;   // entries of the per-step RF table a launch builds (0: none)
     float wscale;       // Boris: (0.5 q/m dt) / hqdt - 1, applied to each velocity increment
     int32_t k_elems;    // map elements per z cell: the record width, 0 when the map does not vary along z
+    uint32_t inner_span[3];   // n - 3 per axis (0 below 4 nodes): cells 1 .. n-3 have inner corners only
 };
 
 // The electrode surface of a mixed-form Boris track (a second kernel
