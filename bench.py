@@ -53,7 +53,7 @@ def parse():
                     help="steps per launch once the bunch has left the map (no sorts then)")
     ap.add_argument("--free-chunk", type=int, default=None,
                     help="steps per launch once the bunch is back in row order and met no map "
-                         "(default 4 x --long-chunk)")
+                         "(default 10 x --long-chunk)")
     ap.add_argument("--sort-every", type=int, default=None,
                     help="cell re-sort interval in steps while the map is populated (also the launch length "
                          "then); 0 = never; default 300 for rf_gap (best of a 50-1000 sweep), 100 otherwise "

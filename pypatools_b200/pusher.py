@@ -250,9 +250,10 @@ class DeviceTracker:
         Once a finished launch met no map at all, the particles go back to
         row order (``restore_order``) for the snapshot rows' sake, until a
         map holds particles again; launches in row order with no map met take
-        ``free_chunk`` steps (default 4 ``long_chunk``): their field-free runs
+        ``free_chunk`` steps (default 10 ``long_chunk``): their field-free runs
         cost little, so the state read and written per launch is what a
-        longer launch saves.
+        longer launch saves, while the counters still come back often enough
+        to notice a bunch that meets a map again.
         ``after_launch(steps_done)`` runs after each launch is enqueued;
         ``launch_events`` (a list) receives (start event, end event, first
         step, steps) for each track launch."""
@@ -261,7 +262,7 @@ class DeviceTracker:
         chunk = max(1, int(chunk))
         adaptive = sort_every > 0 and self.dfields.has_maps and self.n > 0
         long_chunk = max(chunk, int(long_chunk or 10 * max(sort_every, 1)))
-        free_chunk = max(long_chunk, int(free_chunk or 4 * long_chunk))
+        free_chunk = max(long_chunk, int(free_chunk or 10 * long_chunk))
         st = torch.cuda.current_stream(self.device) if stream is None else stream
         if adaptive and self.counters is None:
             self.counters = torch.zeros(2, dtype=torch.int64, device=self.device)
