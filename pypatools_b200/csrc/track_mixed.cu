@@ -797,7 +797,11 @@ __device__ __forceinline__ void drift_quanta(const Drift& d, float2 Q[3], float2
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float bound = fmaf((float)kCarry, fabsf(d.dh[a]), 2.0f);
-        const int eb = (__float_as_int(bound) >> 23) & 0xff;   // bound in [2^(eb-127), 2^(eb-126))
+        // bound in [2^(eb-127), 2^(eb-126)); held to u <= 1 cell (carry_periods'
+        // shifts), which only increments of 2^19 cells per step and more reach:
+        // those leave the 2^24-cell range within a carry period, where the
+        // launch's range check flags them
+        const int eb = min((__float_as_int(bound) >> 23) & 0xff, 150);
         const float u = __int_as_float((eb - 23) << 23);        // float32 spacing below 2^(eb-126)
         const float ui = __int_as_float((277 - eb) << 23);      // 1 / u (both powers of two)
         const float q = rintf(d.dh[a] * ui) * u;
