@@ -835,10 +835,10 @@ __device__ __forceinline__ void carry(float cf[3], float2 o[3], const float2 U[3
 // period's kCarry r an integer R; a carry moves floor((L + R) / 2^19) quanta u
 // into the high word and leaves (L + R) mod 2^19, so after N periods the low
 // word is (L0 + N R) mod 2^19 and the quanta moved sum to
-// floor((L0 + N R) / 2^19).  In units of u (u = 2^-s) the high word H gains
+// floor((L0 + N R) / 2^19).  In units of u (u = 2^-sh) the high word H gains
 // kCarry q / u and the moved quanta each period, and each carry takes the
 // whole cells out of it; so after the last carry the cells moved out are
-// floor((A - Kp) / 2^s), with A the high word's total and Kp the last
+// floor((A - Kp) / 2^sh), with A the high word's total and Kp the last
 // period's quanta, and the high word keeps the rest of A.  All of it is exact
 // integer arithmetic on exact conversions, so the result has the bits of the
 // N periods taken one by one.
@@ -934,7 +934,7 @@ __device__ __forceinline__ void drift_steps(float cf[3], float2 o[3], const floa
         carry_periods(cf, o, Q, U, np);
         j += np * kCarry;
     }
-    if (j < m) run(m - j);   // fewer than kCarry steps from an aligned start: no carry point
+    if (j < m) run(m - j);   // the steps after the last carry point (fewer than kCarry)
     normalise(cf, o);
 }
 
